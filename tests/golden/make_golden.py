@@ -1,0 +1,166 @@
+"""Generate the golden vectors in tests/golden/ from the compiled reference.
+
+Runs only where the reference sources are available (``make -C oracle ref`` builds
+``oracle/_ref/libmara_ref.so`` from them); the fixtures it writes are committed so that the
+tests need neither the reference nor its build on any other machine.
+
+    python tests/golden/make_golden.py
+
+Fixtures (all float64, AoS primitive layout with 3 guard zones where a grid is involved):
+  step_*.npz      whole-step runs through Mara.advance / Mara.get_timestep
+  c2p.npz         Rmhd::ConsToPrim (ladder) and the two solvers on random states
+  flux.npz        FluxAndEigenvalues on random prims, dims 1..3
+  riemann_*.npz   IntercellFlux of HLL / HLLC / HLLD on random face pairs
+  recon.npz       PLM (theta=2) and WENO5-FV (JS96, B08, SZ10) on random stencils
+  divb.npz        measure.mean_max_divB / max_lorentz_factor on the step fixtures' states
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from ctf_b200 import ics  # noqa: E402
+from oracle import RefOracle, Scheme  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+STEP_CASES = {
+    # name: (scheme kwargs, IC builder, steps, cfl)
+    "plm_hlld_rk2_8": (dict(n=(8, 8, 8)), lambda: ics.turbulence_box((8, 8, 8), seed=11), 6, 0.3),
+    "weno5_hlld_rk3_8": (dict(n=(8, 8, 8), extrap="weno5", advance="rk3"),
+                         lambda: ics.turbulence_box((8, 8, 8), seed=12), 4, 0.3),
+    "plm_hllc_rk3_odd": (dict(n=(9, 7, 5), riemann="hllc", advance="rk3"),
+                         lambda: ics.turbulence_box((9, 7, 5), seed=13), 4, 0.3),
+    "pcm_hll_rk4_6": (dict(n=(6, 6, 6), extrap="pcm", riemann="hll", advance="rk4"),
+                      lambda: ics.turbulence_box((6, 6, 6), seed=14), 3, 0.3),
+    "kh2d_plm_hllc_rk3": (dict(n=(24, 16), x0=(0.0, 0.0), x1=(1.0, 1.0), riemann="hllc",
+                               advance="rk3"), lambda: ics.kh_box((24, 16), seed=15), 5, 0.3),
+    "kh2d_weno5_hlld_rk2": (dict(n=(16, 12), x0=(0.0, 0.0), x1=(1.0, 1.0), extrap="weno5",
+                                 advance="rk2"), lambda: ics.kh_box((16, 12), seed=16), 4, 0.3),
+    "hllc_fail_12": (dict(n=(12, 12, 12), riemann="hllc", advance="rk3"),
+                    lambda: ics.turbulence_box((12, 12, 12), seed=1), 3, 0.3),
+}
+
+
+def step_fixture(name, kw, ic, steps, cfl):
+    scheme = Scheme(**kw)
+    ref = RefOracle(scheme)
+    P0 = ic()
+    P = P0.copy()
+    errs = [ref.advance(P, 0.0)]
+    ml = [ref.max_lambda]
+    dts, states = [], []
+    for _ in range(steps):
+        dt = ref.get_timestep(cfl)
+        dts.append(dt)
+        e = ref.advance(P, dt)
+        errs.append(e)
+        ml.append(ref.max_lambda)
+        states.append(P.copy())
+    divb = [ref.mean_max_divB(s) for s in [P0] + states]
+    wmax = [ref.max_lorentz_factor(s) for s in [P0] + states]
+    ref.close()
+    np.savez_compressed(os.path.join(OUT, f"step_{name}.npz"), P0=P0, states=np.stack(states),
+                        dts=np.array(dts), errors=np.array(errs), max_lambda=np.array(ml),
+                        divb=np.array(divb), wmax=np.array(wmax), cfl=cfl,
+                        scheme=np.array(repr(kw)))
+    print(f"step_{name}: errors {errs}")
+
+
+def random_prims(rng, n, wmax=10.0, sigma_max=10.0, pmin=1e-3):
+    """Random physical prim states spanning low/high Lorentz factor and magnetisation."""
+    rho = np.exp(rng.uniform(np.log(0.1), np.log(10.0), n))
+    pre = np.exp(rng.uniform(np.log(pmin), np.log(10.0), n))
+    W = np.exp(rng.uniform(0, np.log(wmax), n))
+    vdir = rng.standard_normal((n, 3))
+    vdir /= np.linalg.norm(vdir, axis=1, keepdims=True)
+    v = vdir * np.sqrt(1 - 1 / W ** 2)[:, None]
+    h = 1 + 4.0 * pre / rho
+    sigma = np.exp(rng.uniform(np.log(1e-3), np.log(sigma_max), n))
+    bdir = rng.standard_normal((n, 3))
+    bdir /= np.linalg.norm(bdir, axis=1, keepdims=True)
+    B = bdir * np.sqrt(sigma * rho * h)[:, None]
+    return np.concatenate([rho[:, None], pre[:, None], v, B], axis=1)
+
+
+def function_fixtures():
+    rng = np.random.default_rng(2024)
+    ref = RefOracle(Scheme(n=(4, 4, 4)))
+    # c2p ----------------------------------------------------------------------------------
+    P = random_prims(rng, 600)
+    U = np.array([ref.prim_to_cons(p)[0] for p in P])
+    ladder = [ref.cons_to_prim(u, guess=np.zeros(8)) for u in U]
+    guess = P * (1 + 1e-3 * rng.standard_normal(P.shape))
+    solvers = {}
+    for solver in (0, 1):
+        for g in (0, 1):
+            res = [ref.c2p_solve(u, solver, g, pg) for u, pg in zip(U, guess)]
+            solvers[f"P_{solver}{g}"] = np.array([r[0] for r in res])
+            solvers[f"err_{solver}{g}"] = np.array([r[1] for r in res])
+            solvers[f"it_{solver}{g}"] = np.array([r[2] for r in res])
+    np.savez_compressed(os.path.join(OUT, "c2p.npz"), P=P, U=U, guess=guess,
+                        P_ladder=np.array([r[0] for r in ladder]),
+                        err_ladder=np.array([r[1] for r in ladder]), **solvers)
+    # flux + eigenvalues --------------------------------------------------------------------
+    P = random_prims(rng, 400)
+    F = np.zeros((3, len(P), 8))
+    lam = np.zeros((3, len(P), 2))
+    for d in range(3):
+        for i, p in enumerate(P):
+            f, ap, am = ref.flux(p, d + 1)
+            F[d, i] = f
+            lam[d, i] = ap, am
+    np.savez_compressed(os.path.join(OUT, "flux.npz"), P=P, F=F, lam=lam)
+    ref.close()
+    # Riemann solvers ------------------------------------------------------------------------
+    for solver in ("hll", "hllc", "hlld"):
+        ref = RefOracle(Scheme(n=(4, 4, 4), riemann=solver))
+        Pl = random_prims(rng, 300, wmax=3.0, sigma_max=3.0)
+        Pr = Pl * (1 + 0.2 * rng.standard_normal(Pl.shape))
+        Pr[:, 0:2] = np.abs(Pr[:, 0:2])
+        vr = Pr[:, 2:5]
+        sp = np.linalg.norm(vr, axis=1)
+        Pr[:, 2:5] = np.where((sp > 0.95)[:, None], vr * (0.95 / sp)[:, None], vr)
+        Pr[:60, 5] = Pl[:60, 5] = 0.0                            # Bn = 0 faces
+        Pr[60:90, 5:8] = Pl[60:90, 5:8] = Pl[60:90, 5:8] * 1e-9  # near-degenerate field
+        F = np.zeros((3, len(Pl), 8))
+        err = np.zeros((3, len(Pl)), dtype=int)
+        mls = np.zeros((3, len(Pl)))
+        for d in range(3):
+            for i in range(len(Pl)):
+                ref.lib.ref_reset_max_lambda()
+                f, e = ref.riemann(Pl[i], Pr[i], d + 1)
+                F[d, i] = f
+                err[d, i] = e
+                mls[d, i] = ref.max_lambda
+        np.savez_compressed(os.path.join(OUT, f"riemann_{solver}.npz"), Pl=Pl, Pr=Pr, F=F,
+                            err=err, max_lambda=mls)
+        ref.close()
+    # reconstruction ------------------------------------------------------------------------
+    V = rng.standard_normal((500, 5))
+    V[:100] = np.cumsum(np.abs(V[:100]), axis=1)      # monotone stencils
+    V[100:150, 2] += 10.0                              # extrema
+    out = {"V": V}
+    for IS in ("js96", "b08", "sz10"):
+        ref = RefOracle(Scheme(n=(4, 4, 4), extrap="weno5", IS=IS))
+        out[f"weno_c2r_{IS}"] = np.array([ref.reconstruct(v, 4) for v in V])
+        out[f"weno_c2l_{IS}"] = np.array([ref.reconstruct(v, 5) for v in V])
+        ref.close()
+    ref = RefOracle(Scheme(n=(4, 4, 4), theta=2.0))
+    out["plm_c2r"] = np.array([ref.reconstruct(v, 1) for v in V])
+    out["plm_c2l"] = np.array([ref.reconstruct(v, 0) for v in V])
+    ref.close()
+    np.savez_compressed(os.path.join(OUT, "recon.npz"), **out)
+
+
+if __name__ == "__main__":
+    for name, (kw, ic, steps, cfl) in STEP_CASES.items():
+        step_fixture(name, kw, ic, steps, cfl)
+    function_fixtures()
+    total = sum(os.path.getsize(os.path.join(OUT, f)) for f in os.listdir(OUT) if f.endswith(".npz"))
+    print(f"wrote {total / 1e6:.2f} MB of fixtures")

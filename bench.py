@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 RMHD step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
+
+A step is one full Mara advance (all RK stages) of a seeded synthetic box.  The headline
+workload is the 256^3 relativistic-MHD turbulence box (rho = p = 1, Gamma 4/3, Gaussian
+random velocity with per-mode power ~ |k|^-2 on 1 <= |k| <= 4, rms 0.3c, |v| < 0.9;
+B = (0, 0, 1) + solenoidal perturbation of rms 0.1) with component-wise WENO5 + HLLD + RK3 +
+flux-CT, CFL 0.3.  `value` is the FP32-bulk path (FP64 c2p polish, magnetic field and dt);
+the plain FP64 path runs the same steps in the same call and is reported beside it, with the
+relative L1 difference of every primitive between the two after the timed steps.
+
+Both precisions advance with the same fixed dt (CFL 0.3 of the primed MaxLambda) so their
+final states are comparable.  Every array (1.2 GB per FP64 state at 256^3) is larger than
+the 126 MB L2, so no flush is needed between steps.  For N > 1 (torchrun) every rank
+advances its own box: independent replicas, weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RMHD zone-updates/s on 1 B200: FP32+learned c2p vs plain FP64 at stated L1 err"
+UNIT = "zone-updates/s"
+
+WORKLOADS = {
+    # name: (n, ic, scheme kwargs)
+    "turb256_weno5_hlld_rk3": ((256, 256, 256), "turbulence",
+                               dict(extrap="weno5", riemann="hlld", advance="rk3")),
+    "turb64_plm_hlld_rk2": ((64, 64, 64), "turbulence", dict(extrap="plm", riemann="hlld", advance="rk2")),
+    "turb512_plm_hlld_rk3": ((512, 512, 512), "turbulence",
+                             dict(extrap="plm", riemann="hlld", advance="rk3")),
+    "turb128_weno5_hlld_rk3": ((128, 128, 128), "turbulence",
+                               dict(extrap="weno5", riemann="hlld", advance="rk3")),
+}
+DEFAULT_WORKLOAD = "turb256_weno5_hlld_rk3"
+CFL = 0.3
+
+
+def make_ic(kind, n, seed=0):
+    from ctf_b200 import ics
+    if kind == "turbulence":
+        return ics.turbulence_box(n, seed=seed)
+    if kind == "stress":
+        return ics.stress_box(n, seed=seed)
+    raise ValueError(kind)
+
+
+def launches_per_step(nd, rk):
+    ns = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}[rk]
+    return 2 + ns * (2 + nd) + 2
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def time_device(solver, steps, warmup, dt, torch, stream):
+    """Warm up, then time `steps` advances with CUDA events on the solver's stream."""
+    solver.advance_async(warmup, dt=dt)
+    solver.synchronize()
+    solver.profile_read()   # drop warm-up launches
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    solver.advance_async(steps, dt=dt)
+    end.record(stream)
+    end.synchronize()
+    ms = start.elapsed_time(end)
+    prof = solver.profile_read()
+    return ms, prof
+
+
+def rel_l1(a, b, nd, ng=3):
+    sl = tuple(slice(ng, -ng) if d < nd else slice(None) for d in range(3))
+    a, b = a[sl], b[sl]
+    out = {}
+    for q, name in enumerate(["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]):
+        den = np.abs(b[..., q]).mean()
+        num = np.abs(a[..., q] - b[..., q]).mean()
+        out[name] = float(num / den) if den > 0 else float(num)
+    return out
+
+
+def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0):
+    """Time the reference's CPU advance (or the C restatement) on a bounded sample box."""
+    from oracle import PortOracle, REF_SO, RefOracle, Scheme
+    sch = Scheme(n=(n, n, n), **scheme_kw)
+    kind = "reference" if (use_ref and os.path.exists(REF_SO)) else "port"
+    o = RefOracle(sch) if kind == "reference" else PortOracle(sch)
+    P = make_ic("turbulence", (n, n, n), seed=seed)
+    o.advance(P, 0.0)
+    dt = o.get_timestep(CFL)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.advance(P, dt)
+    sec = time.perf_counter() - t0
+    if kind == "reference":
+        o.close()
+    return kind, n ** 3 * steps / sec, sec
+
+
+def _cpu_worker(args):
+    scheme_kw, steps, n, seed = args
+    return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed)
+
+
+def run_reference_arm(args, wl_name, rank, world):
+    """--impl reference: the reference's own CPU advance on every host core (independent
+    replicas of a 64^3 sample box of the workload's scheme)."""
+    if rank != 0:
+        return
+    n_wl, _, scheme_kw = WORKLOADS[wl_name]
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    n = 64 if n_wl[0] >= 64 else n_wl[0]
+    steps = args.steps
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s) for s in range(cores)])
+    wall = time.perf_counter() - t0
+    kind = res[0][0]
+    value = float(sum(r[1] for r in res))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": float(np.mean([r[2] for r in res]) / steps * 1e3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl_name, "sample": f"{cores} replicas of a {n}^3 box, same scheme",
+                   "scheme": scheme_kw, "cfl": CFL},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{cores} concurrent replicas x {steps} steps of a {n}^3 turbulence "
+                                   f"box ({scheme_kw}), interior zone-updates/s summed; wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, args.workload, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+
+    from ctf_b200.mara import Scheme, Solver
+
+    n, ic_kind, scheme_kw = WORKLOADS[args.workload]
+    P0 = make_ic(ic_kind, n, seed=rank)
+    stream = torch.cuda.Stream()
+    results = {}
+    states = {}
+    precisions = ["fp32"] if args.skip_fp64 else ["fp32", "fp64"]
+    dt_fixed = None
+    for prec in reversed(precisions):   # FP64 first: its primed MaxLambda sets the shared dt
+        s = Solver(Scheme(precision=prec, **scheme_kw), n, stream=stream.cuda_stream)
+        s.upload(P0)
+        assert s.advance(0.0) == 0, "priming advance failed"
+        if dt_fixed is None:
+            dt_fixed = s.get_timestep(CFL)
+        s.upload(P0)
+        s.profile_enable(capacity=launches_per_step(len(n), scheme_kw["advance"]) * (args.steps + args.warmup) + 64)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            ms, prof = time_device(s, args.steps, args.warmup, dt_fixed, torch, stream)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        st = s.stats()
+        zones = int(np.prod(n))
+        results[prec] = {"ms_total": ms, "ms_per_step": ms / args.steps,
+                         "value": zones * args.steps * world / (ms * 1e-3), "prof": prof, "stats": st,
+                         "clocks": clk.summary()}
+        states[prec] = s.download()
+        s.profile_disable()
+        if prec == "fp32":
+            solver_fp32 = s
+        else:
+            s.close()
+
+    head = results["fp32"]
+    out = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL,
+                   "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt",
+                   "dt": dt_fixed, "l2": "every state array > 126 MB L2 (no flush needed)",
+                   "parallelism": f"{world} independent replica(s)"},
+        "gpu_launches": launches_per_step(len(n), scheme_kw["advance"]) * args.steps,
+        "clocks": head["clocks"],
+    }
+    if "fp64" in results:
+        out["fp64_plain"] = {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
+                             "clocks": results["fp64"]["clocks"]}
+        out["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
+        out["l1_rel_vs_fp64"] = rel_l1(states["fp32"], states["fp64"], len(n))
+
+    # roofline of the dominant kernel (event-timed inside the timed region)
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    prof = head["prof"]
+    dom = max(("flux", "update", "c2p", "p2c"), key=lambda k: prof[k]["ms"])
+    tsz = 4
+    per_unit = {"flux": 16 * tsz,                       # read 8 face-state comps, write 8 flux comps
+                "update": 5 * tsz * 3 + 3 * 8 * 3 + 3 * 8 * tsz,   # Un, Us, Uout (44 B each) + F,G,H
+                "c2p": 44 + 8 * tsz,                    # read U (44 B), write 8 prim comps
+                "p2c": 44 + 44}
+    d = prof[dom]
+    alg_bytes_per_launch = per_unit[dom] * d["units"] / max(d["launches"], 1)
+    avg_ms = d["ms"] / max(d["launches"], 1)
+    achieved = alg_bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                       "frac": achieved / hbm, "traffic": None,
+                       "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                       "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
+                       "algorithmic_bytes_per_unit": per_unit[dom]}
+    out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "face_c2p_calls",
+                                                      "face_c2p_iters", "hlld_ok", "hlld_hllc", "pcm_retry")}
+
+    # end to end through Mara.advance(buf, dt) semantics with pinned host buffers
+    if not args.no_e2e:
+        import torch as _t
+        host = _t.empty(solver_fp32.shape, dtype=_t.float64, pin_memory=True).numpy()
+        host[...] = P0
+        for _ in range(max(1, args.warmup)):
+            solver_fp32.advance_host(host, dt_fixed)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            dt = solver_fp32.get_timestep(CFL)
+            _, e = solver_fp32.advance_host(host, min(dt, dt_fixed))
+        sec = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([sec], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            sec = float(t.item())
+        nbytes = int(np.prod(solver_fp32.shape)) * 8
+        out["e2e"] = {"value": int(np.prod(n)) * args.steps * world / sec, "unit": UNIT,
+                      "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                      "api": "mgpu_advance_host (Mara.advance(buf, dt)) + mgpu_get_timestep"}
+    solver_fp32.close()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, v, sec = cpu_sample(scheme_kw, steps=2, n=48)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                               "sample": f"48^3 turbulence box, same scheme, 2 steps after priming "
+                                         f"({sec:.1f} s), interior zone-updates/s on 1 core"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

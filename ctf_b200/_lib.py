@@ -1,0 +1,97 @@
+"""ctypes binding of libmaragpu.so (the C ABI in include/mara_gpu.h).
+
+The library is built in-tree (``make -C ctf_b200/csrc``).  There is no fallback: if the
+shared library is missing and cannot be built, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmaragpu.so")
+CSRC = os.path.join(HERE, "csrc")
+
+_lock = threading.Lock()
+_lib = None
+
+
+class MgpuConfig(ctypes.Structure):
+    _fields_ = [("fluid", ctypes.c_int), ("gamma", ctypes.c_double), ("recon", ctypes.c_int),
+                ("theta", ctypes.c_double), ("is_mode", ctypes.c_int), ("sz10A", ctypes.c_double),
+                ("riemann", ctypes.c_int), ("rk", ctypes.c_int), ("pfloor", ctypes.c_double),
+                ("ereset", ctypes.c_int), ("preset", ctypes.c_double), ("dreset", ctypes.c_double),
+                ("precision", ctypes.c_int), ("learned_c2p", ctypes.c_int)]
+
+
+class MgpuStats(ctypes.Structure):
+    _fields_ = [("max_lambda", ctypes.c_double), ("dt", ctypes.c_double), ("errors", ctypes.c_int),
+                ("committed", ctypes.c_int), ("c2p_calls", ctypes.c_ulonglong),
+                ("c2p_iters", ctypes.c_ulonglong), ("c2p_attempt", ctypes.c_ulonglong * 6),
+                ("face_c2p_calls", ctypes.c_ulonglong), ("face_c2p_iters", ctypes.c_ulonglong),
+                ("hlld_ok", ctypes.c_ulonglong), ("hlld_hllc", ctypes.c_ulonglong),
+                ("pcm_retry", ctypes.c_ulonglong)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "c2p_attempt"}
+        d["c2p_attempt"] = list(self.c2p_attempt)
+        return d
+
+
+# exported symbol -> (restype, argtypes)
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+SIGNATURES = {
+    "mgpu_default_config": (ctypes.c_int, [ctypes.POINTER(MgpuConfig)]),
+    "mgpu_create": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), ctypes.POINTER(_vp)]),
+    "mgpu_destroy": (ctypes.c_int, [_vp]),
+    "mgpu_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "mgpu_last_error": (ctypes.c_char_p, [_vp]),
+    "mgpu_set_domain": (ctypes.c_int, [_vp, _dp, _dp, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "mgpu_num_zones": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_upload_prim": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_download_prim": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_upload_prim_device": (ctypes.c_int, [_vp, _vp]),
+    "mgpu_download_prim_device": (ctypes.c_int, [_vp, _vp]),
+    "mgpu_advance": (ctypes.c_int, [_vp, ctypes.c_double, _ip]),
+    "mgpu_advance_host": (ctypes.c_int, [_vp, _dp, ctypes.c_double, _dp, _ip]),
+    "mgpu_advance_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double]),
+    "mgpu_synchronize": (ctypes.c_int, [_vp]),
+    "mgpu_get_timestep": (ctypes.c_int, [_vp, ctypes.c_double, _dp]),
+    "mgpu_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuStats)]),
+    "mgpu_set_primitive": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_divB": (ctypes.c_int, [_vp, _dp, _dp]),
+    "mgpu_max_lorentz_factor": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "mgpu_profile_disable": (ctypes.c_int, [_vp]),
+    "mgpu_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_set_c2p_network": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_longlong]),
+}
+
+
+def build(force: bool = False) -> str:
+    """Compile libmaragpu.so for sm_100a with nvcc (no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", CSRC, "-j4"], check=True)
+    return LIB_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (building it first if it is absent); raises if that fails."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                build()
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+        return _lib

@@ -1,0 +1,681 @@
+// Host side of libmaragpu.so: the solver handle, device buffers, transfers, measures and the
+// C ABI declared in include/mara_gpu.h.  Kernels live in kernels_fp64.cu (compiled with
+// --fmad=false) and kernels_fp32.cu.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "../../include/mara_gpu.h"
+#include "rmhd_types.cuh"
+
+MGPU_DECLARE_PRECISION(fp64)
+MGPU_DECLARE_PRECISION(fp32)
+
+using namespace mgpu;
+
+struct mgpu_solver {
+  mgpu_config cfg;
+  std::string err;
+  bool have_domain = false;
+  Grid g{};
+  double x0[3] = {0, 0, 0}, x1[3] = {1, 1, 1};
+  double min_dx = 1.0;
+  int N[3] = {1, 1, 1};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  AdvanceBuffers b{};
+  std::vector<void *> allocations;
+  Ctl *ctl = nullptr;           // device
+  Ctl *ctl_host = nullptr;      // pinned mirror
+  double *staging = nullptr;    // device AoS staging for host transfers
+  long long staging_zones = 0;
+  double *red = nullptr;        // reduction partials (device)
+  double *red_host = nullptr;   // pinned
+  float *mlp = nullptr;         // learned c2p network (device)
+  long long mlp_count = 0;
+  // kernel timing
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_tag;
+  std::vector<long long> prof_units;
+  int prof_count = 0;
+  LaunchProfiler prof{};
+  bool prof_on = false;
+};
+
+namespace {
+
+constexpr int RED_BLOCKS = 1184;   // 148 SMs x 8
+
+int fail(mgpu_solver *h, int code, const std::string &msg)
+{
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(mgpu_solver *h, cudaError_t e, const char *where)
+{
+  return fail(h, MGPU_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                               \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);     \
+  } while (0)
+
+bool fp32(const mgpu_solver *h) { return h->cfg.precision == MGPU_PREC_FP32; }
+
+PhysParams phys(const mgpu_solver *h)
+{
+  PhysParams p;
+  p.gamma = h->cfg.gamma;
+  p.pfloor = h->cfg.pfloor;
+  p.theta = h->cfg.theta;
+  p.sz10A = h->cfg.sz10A;
+  p.is_mode = h->cfg.is_mode;
+  p.recon = h->cfg.recon;
+  p.riemann = h->cfg.riemann;
+  p.learned = h->cfg.learned_c2p && h->mlp != nullptr;
+  p.mlp = h->mlp;
+  return p;
+}
+
+void free_buffers(mgpu_solver *h)
+{
+  for (void *p : h->allocations) cudaFree(p);
+  h->allocations.clear();
+  h->b = AdvanceBuffers{};
+  h->staging = nullptr;
+  h->red = nullptr;
+}
+
+cudaError_t dalloc(mgpu_solver *h, void **p, size_t bytes)
+{
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) {
+    h->allocations.push_back(*p);
+    e = cudaMemsetAsync(*p, 0, bytes, h->stream);
+  }
+  return e;
+}
+
+TransferArgs transfer_args(mgpu_solver *h)
+{
+  TransferArgs t;
+  t.g = h->g;
+  t.b = h->b;
+  t.ctl = h->ctl;
+  t.stream = h->stream;
+  return t;
+}
+
+int ensure_ready(mgpu_solver *h)
+{
+  if (!h) return MGPU_ERR_ARG;
+  if (!h->have_domain) return fail(h, MGPU_ERR_STATE, "need a domain to run this, use set_domain");
+  return MGPU_OK;
+}
+
+// ---- measures (Mara/mara.cpp:2232-2324) on an 8 x T face array ------------------------------
+template <class T>
+__global__ void k_divB(Grid g, const T *P, double *partial)
+{
+  // corner-centred divergence over i in [ng, G0-ng-1) etc. (interior corners but the last)
+  const int ng = g.ng;
+  const long long ni = g.G[0] - 2 * ng - 1;
+  const long long nj = g.nd >= 2 ? g.G[1] - 2 * ng - 1 : 1;
+  const long long nk = g.nd >= 3 ? g.G[2] - 2 * ng - 1 : 1;
+  const long long total = (ni > 0 && nj > 0 && nk > 0) ? ni * nj * nk : 0;
+  double sum = 0.0, mx = -INFINITY;
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long) gridDim.x * blockDim.x) {
+    const int i = ng + (int) (t / (nj * nk));
+    const int j = (g.nd >= 2 ? ng : 0) + (int) ((t / nk) % nj);
+    const int k = (g.nd >= 3 ? ng : 0) + (int) (t % nk);
+    auto B = [&](int q, int a, int b, int c) {
+      return double(P[(long long) q * g.cs + ((long long) a * g.G[1] + b) * g.G[2] + c]);
+    };
+    double d;
+    if (g.nd == 2) {
+      d = (B(5, i + 1, j, 0) + B(5, i + 1, j + 1, 0) - B(5, i, j, 0) - B(5, i, j + 1, 0)) / 2.0 +
+          (B(6, i, j + 1, 0) + B(6, i + 1, j + 1, 0) - B(6, i, j, 0) - B(6, i + 1, j, 0)) / 2.0;
+    } else {
+      d = ((B(5, i + 1, j, k) + B(5, i + 1, j + 1, k) + B(5, i + 1, j, k + 1) + B(5, i + 1, j + 1, k + 1)) -
+           (B(5, i, j, k) + B(5, i, j + 1, k) + B(5, i, j, k + 1) + B(5, i, j + 1, k + 1))) / 4.0 +
+          ((B(6, i, j + 1, k) + B(6, i, j + 1, k + 1) + B(6, i + 1, j + 1, k) + B(6, i + 1, j + 1, k + 1)) -
+           (B(6, i, j, k) + B(6, i, j, k + 1) + B(6, i + 1, j, k) + B(6, i + 1, j, k + 1))) / 4.0 +
+          ((B(7, i, j, k + 1) + B(7, i + 1, j, k + 1) + B(7, i, j + 1, k + 1) + B(7, i + 1, j + 1, k + 1)) -
+           (B(7, i, j, k) + B(7, i + 1, j, k) + B(7, i, j + 1, k) + B(7, i + 1, j + 1, k))) / 4.0;
+    }
+    sum += d;
+    mx = fmax(mx, d);
+  }
+  __shared__ double ss[256], sm[256];
+  ss[threadIdx.x] = sum;
+  sm[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = ss[0];
+    partial[2 * blockIdx.x + 1] = sm[0];
+  }
+}
+
+template <class T>
+__global__ void k_wmax(Grid g, const T *P, double *partial)
+{
+  double mx = 0.0;
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < g.ninterior;
+       t += (long long) gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_coords(g, t, i, j, k);
+    const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+    const double v0 = double(P[2 * g.cs + z]), v1 = double(P[3 * g.cs + z]), v2 = double(P[4 * g.cs + z]);
+    const double W0 = 1.0 / sqrt(1.0 - (v0 * v0 + v1 * v1 + v2 * v2));
+    mx = fmax(mx, W0);
+  }
+  __shared__ double sm[256];
+  sm[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+}  // namespace
+
+static void prof_free(mgpu_solver *h)
+{
+  for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
+  h->prof_ev.clear();
+  h->prof_tag.clear();
+  h->prof_units.clear();
+  h->prof_on = false;
+}
+
+
+extern "C" {
+
+int mgpu_default_config(mgpu_config *c)
+{
+  if (!c) return MGPU_ERR_ARG;
+  memset(c, 0, sizeof(*c));
+  c->fluid = MGPU_FLUID_RMHD;
+  c->gamma = 4.0 / 3.0;
+  c->recon = MGPU_RECON_PLM;
+  c->theta = 2.0;
+  c->is_mode = MGPU_IS_JS96;
+  c->sz10A = 50.0;
+  c->riemann = MGPU_RIEMANN_HLLD;
+  c->rk = 2;
+  c->pfloor = -1.0;
+  c->ereset = 0;
+  c->preset = 1.0;
+  c->dreset = 1.0;
+  c->precision = MGPU_PREC_FP64;
+  c->learned_c2p = 0;
+  return MGPU_OK;
+}
+
+static int check_config(mgpu_solver *h, const mgpu_config *c)
+{
+  if (c->fluid != MGPU_FLUID_RMHD) return fail(h, MGPU_ERR_UNSUPPORTED, "only the 'rmhd' fluid is provided");
+  if (!(c->gamma > 1.0)) return fail(h, MGPU_ERR_ARG, "gamma-law index must exceed 1");
+  if (c->recon < 0 || c->recon > 2) return fail(h, MGPU_ERR_ARG, "no such extrap");
+  if (c->riemann < 0 || c->riemann > 2) return fail(h, MGPU_ERR_ARG, "no such riemann solver");
+  if (c->rk < 1 || c->rk > 4) return fail(h, MGPU_ERR_ARG, "no such advance option");
+  if (c->is_mode < 0 || c->is_mode > 2) return fail(h, MGPU_ERR_ARG, "no such IS");
+  if (c->precision != MGPU_PREC_FP64 && c->precision != MGPU_PREC_FP32)
+    return fail(h, MGPU_ERR_ARG, "no such precision");
+  return MGPU_OK;
+}
+
+int mgpu_create(const mgpu_config *cfg, mgpu_solver **out)
+{
+  if (!out) return MGPU_ERR_ARG;
+  *out = nullptr;
+  mgpu_solver *h = new mgpu_solver;
+  if (cfg) h->cfg = *cfg;
+  else mgpu_default_config(&h->cfg);
+  int rc = check_config(h, &h->cfg);
+  if (rc) {
+    fprintf(stderr, "[mgpu] %s\n", h->err.c_str());
+    delete h;
+    return rc;
+  }
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void **) &h->ctl, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaMallocHost((void **) &h->ctl_host, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaMallocHost((void **) &h->red_host, sizeof(double) * 2 * RED_BLOCKS);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[mgpu] CUDA unavailable: %s\n", cudaGetErrorString(e));
+    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->ctl) cudaFree(h->ctl);
+    if (h->ctl_host) cudaFreeHost(h->ctl_host);
+    delete h;
+    return MGPU_ERR_CUDA;
+  }
+  h->own_stream = true;
+  *out = h;
+  return MGPU_OK;
+}
+
+int mgpu_destroy(mgpu_solver *h)
+{
+  if (!h) return MGPU_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  prof_free(h);
+  if (h->mlp) cudaFree(h->mlp);
+  if (h->ctl) cudaFree(h->ctl);
+  if (h->ctl_host) cudaFreeHost(h->ctl_host);
+  if (h->red_host) cudaFreeHost(h->red_host);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return MGPU_OK;
+}
+
+int mgpu_set_stream(mgpu_solver *h, void *stream)
+{
+  if (!h) return MGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  if (stream) {
+    h->stream = (cudaStream_t) stream;
+    h->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return MGPU_OK;
+}
+
+const char *mgpu_last_error(const mgpu_solver *h) { return h ? h->err.c_str() : "null handle"; }
+
+int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const int *N, int nd, int nq, int ng)
+{
+  if (!h || !x0 || !x1 || !N) return MGPU_ERR_ARG;
+  if (nd < 1 || nd > 3) return fail(h, MGPU_ERR_ARG, "domain must have 1, 2 or 3 dimensions");
+  if (nq != 8) return fail(h, MGPU_ERR_ARG, "the rmhd fluid has Nq = 8");
+  if (ng < 3) return fail(h, MGPU_ERR_ARG, "the step's stencils need Ng >= 3");
+  for (int d = 0; d < nd; ++d)
+    if (N[d] < ng) return fail(h, MGPU_ERR_ARG, "periodic guard fill needs N >= Ng on every axis");
+  CK(cudaStreamSynchronize(h->stream));
+  free_buffers(h);
+  h->have_domain = false;
+  Grid &g = h->g;
+  g = Grid{};
+  g.nd = nd;
+  g.ng = ng;
+  for (int d = 0; d < 3; ++d) {
+    h->N[d] = d < nd ? N[d] : 1;
+    h->x0[d] = d < nd ? x0[d] : 0.0;
+    h->x1[d] = d < nd ? x1[d] : 1.0;
+    g.n[d] = h->N[d];
+    g.G[d] = d < nd ? N[d] + 2 * ng : 1;
+  }
+  g.nz = (long long) g.G[0] * g.G[1] * g.G[2];
+  g.cs = (g.nz + 31) / 32 * 32;
+  g.s[0] = (long long) g.G[1] * g.G[2];
+  g.s[1] = g.G[2];
+  g.s[2] = 1;
+  // GodunovOperator::prepare_integration (Mara/hydro.cpp:80-110)
+  double dd[3];
+  for (int d = 0; d < 3; ++d) dd[d] = (h->x1[d] - h->x0[d]) / (g.G[d] - 2 * ng);
+  g.dx = dd[0];
+  g.dy = dd[1];
+  g.dz = dd[2];
+  g.ninterior = (long long) g.n[0] * g.n[1] * g.n[2];
+  // SimpleCartesianDomain min_dx (Mara/simple-cart.cpp:20-24)
+  h->min_dx = h->x1[0] - h->x0[0];
+  for (int d = 0; d < nd; ++d) {
+    const double dx = (h->x1[d] - h->x0[d]) / h->N[d];
+    if (dx < h->min_dx) h->min_dx = dx;
+  }
+
+  const size_t tsz = fp32(h) ? sizeof(float) : sizeof(double);
+  const size_t cs = (size_t) g.cs;
+  auto state = [&](void **bulk, double **B) -> cudaError_t {
+    cudaError_t e = dalloc(h, bulk, 5 * cs * tsz);
+    if (e == cudaSuccess) e = dalloc(h, (void **) B, 3 * cs * sizeof(double));
+    return e;
+  };
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = state(&h->b.Pc_bulk[i], &h->b.Pc_B[i]);
+  if (e == cudaSuccess) e = state(&h->b.U0_bulk, &h->b.U0_B);
+  if (e == cudaSuccess) e = state(&h->b.U1_bulk, &h->b.U1_B);
+  if (h->cfg.rk == 4)
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = state(&h->b.K_bulk[i], &h->b.K_B[i]);
+  if (e == cudaSuccess) e = dalloc(h, &h->b.PA, 8 * cs * tsz);
+  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+    if (d < nd) e = dalloc(h, &h->b.F[d], 8 * cs * tsz);
+    else h->b.F[d] = h->b.F[0];
+  }
+  h->staging_zones = g.nz < (1ll << 22) ? g.nz : (1ll << 22);   // up to 256 MB of AoS
+  if (e == cudaSuccess) e = dalloc(h, (void **) &h->staging, (size_t) h->staging_zones * 8 * sizeof(double));
+  if (e == cudaSuccess) e = dalloc(h, (void **) &h->red, sizeof(double) * 2 * RED_BLOCKS);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctl, 0, sizeof(Ctl), h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    free_buffers(h);
+    cudaGetLastError();
+    return fail(h, e == cudaErrorMemoryAllocation ? MGPU_ERR_NOMEM : MGPU_ERR_CUDA,
+                std::string("set_domain: ") + cudaGetErrorString(e));
+  }
+  h->have_domain = true;
+  return MGPU_OK;
+}
+
+int mgpu_num_zones(const mgpu_solver *h, long long *nz)
+{
+  if (!h || !nz) return MGPU_ERR_ARG;
+  if (!h->have_domain) return MGPU_ERR_STATE;
+  *nz = h->g.nz;
+  return MGPU_OK;
+}
+
+static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_out, int kind)
+{
+  // kind 0: upload committed state, 1: download committed state, 2: upload PA, 3: download PA
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  const TransferArgs t = transfer_args(h);
+  const long long nz = h->g.nz;
+  const bool upload = kind == 0 || kind == 2;
+  if (dev_in || dev_out) {
+    double *d = (double *) (dev_in ? const_cast<void *>(dev_in) : dev_out);
+    cudaError_t e;
+    if (kind == 0) e = fp32(h) ? upload_fp32(t, d, 0, nz) : upload_fp64(t, d, 0, nz);
+    else if (kind == 1) e = fp32(h) ? download_fp32(t, d, 0, nz) : download_fp64(t, d, 0, nz);
+    else e = fp32(h) ? face_io_fp32(t, d, 0, nz, kind == 3) : face_io_fp64(t, d, 0, nz, kind == 3);
+    CK(e);
+    CK(cudaStreamSynchronize(h->stream));
+    return MGPU_OK;
+  }
+  for (long long z0 = 0; z0 < nz; z0 += h->staging_zones) {
+    const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
+    const size_t bytes = (size_t) cnt * 8 * sizeof(double);
+    if (upload) {
+      CK(cudaMemcpyAsync(h->staging, host + z0 * 8, bytes, cudaMemcpyHostToDevice, h->stream));
+      cudaError_t e = kind == 0 ? (fp32(h) ? upload_fp32(t, h->staging, z0, cnt) : upload_fp64(t, h->staging, z0, cnt))
+                                : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 0)
+                                           : face_io_fp64(t, h->staging, z0, cnt, 0));
+      CK(e);
+    } else {
+      cudaError_t e = kind == 1 ? (fp32(h) ? download_fp32(t, h->staging, z0, cnt)
+                                           : download_fp64(t, h->staging, z0, cnt))
+                                : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 1)
+                                           : face_io_fp64(t, h->staging, z0, cnt, 1));
+      CK(e);
+      CK(cudaMemcpyAsync(host + z0 * 8, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+int mgpu_upload_prim(mgpu_solver *h, const double *host_aos)
+{
+  if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
+  return transfer(h, const_cast<double *>(host_aos), nullptr, nullptr, 0);
+}
+int mgpu_download_prim(mgpu_solver *h, double *host_aos)
+{
+  if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
+  return transfer(h, host_aos, nullptr, nullptr, 1);
+}
+int mgpu_upload_prim_device(mgpu_solver *h, const void *dev_aos)
+{
+  if (!dev_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
+  return transfer(h, nullptr, dev_aos, nullptr, 0);
+}
+int mgpu_download_prim_device(mgpu_solver *h, void *dev_aos)
+{
+  if (!dev_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
+  return transfer(h, nullptr, nullptr, dev_aos, 1);
+}
+int mgpu_set_primitive(mgpu_solver *h, const double *host_aos)
+{
+  if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
+  return transfer(h, const_cast<double *>(host_aos), nullptr, nullptr, 2);
+}
+
+static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
+{
+  AdvanceArgs A;
+  A.g = h->g;
+  A.pp = phys(h);
+  A.rk = h->cfg.rk;
+  A.ereset = h->cfg.ereset;
+  A.preset = h->cfg.preset;
+  A.dreset = h->cfg.dreset;
+  A.dt_mode = dt_mode;
+  A.dt = dt;
+  A.cfl = cfl;
+  A.min_dx = h->min_dx;
+  A.b = h->b;
+  A.ctl = h->ctl;
+  A.stream = h->stream;
+  A.prof = h->prof_on ? &h->prof : nullptr;
+  cudaError_t e = fp32(h) ? advance_fp32(A) : advance_fp64(A);
+  CK(e);
+  return MGPU_OK;
+}
+
+static int read_ctl(mgpu_solver *h)
+{
+  CK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+static int errors_of(const Ctl &c, int rk)
+{
+  const int ns = num_stages(rk);
+  for (int s = 0; s < ns; ++s)
+    if (c.stage_err[s]) return c.stage_err[s];
+  return c.final_err;
+}
+
+int mgpu_advance(mgpu_solver *h, double dt, int *errors)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  rc = enqueue_advance(h, 0, dt, 0.0);
+  if (rc) return rc;
+  rc = read_ctl(h);
+  if (rc) return rc;
+  if (errors) *errors = errors_of(*h->ctl_host, h->cfg.rk);
+  return MGPU_OK;
+}
+
+int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  const auto t0 = std::chrono::steady_clock::now();
+  rc = mgpu_upload_prim(h, host_aos);
+  if (rc) return rc;
+  int err = 0;
+  rc = mgpu_advance(h, dt, &err);
+  if (rc) return rc;
+  if (err == 0) {
+    rc = mgpu_download_prim(h, host_aos);
+    if (rc) return rc;
+  }
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (kzps) *kzps = 1e-3 * (double) h->g.nz / sec;
+  if (errors) *errors = err;
+  return MGPU_OK;
+}
+
+int mgpu_advance_async(mgpu_solver *h, int n, int dt_mode, double dt, double cfl)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (n < 0 || (dt_mode != 0 && dt_mode != 1)) return fail(h, MGPU_ERR_ARG, "bad advance_async arguments");
+  for (int i = 0; i < n; ++i) {
+    rc = enqueue_advance(h, dt_mode, dt, cfl);
+    if (rc) return rc;
+  }
+  return MGPU_OK;
+}
+
+int mgpu_synchronize(mgpu_solver *h)
+{
+  if (!h) return MGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+int mgpu_get_timestep(mgpu_solver *h, double cfl, double *dt)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  rc = read_ctl(h);
+  if (rc) return rc;
+  double ml;
+  memcpy(&ml, &h->ctl_host->max_lambda_bits, sizeof(double));
+  *dt = cfl * h->min_dx / ml;
+  return MGPU_OK;
+}
+
+int mgpu_get_stats(mgpu_solver *h, mgpu_stats *s)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  rc = read_ctl(h);
+  if (rc) return rc;
+  const Ctl &c = *h->ctl_host;
+  memset(s, 0, sizeof(*s));
+  memcpy(&s->max_lambda, &c.max_lambda_bits, sizeof(double));
+  s->dt = c.dt;
+  s->errors = errors_of(c, h->cfg.rk);
+  s->committed = c.committed;
+  s->c2p_calls = c.c2p_calls;
+  s->c2p_iters = c.c2p_iters;
+  for (int a = 0; a < 6; ++a) s->c2p_attempt[a] = c.c2p_attempt[a];
+  s->face_c2p_calls = c.face_c2p_calls;
+  s->face_c2p_iters = c.face_c2p_iters;
+  s->hlld_ok = c.hlld_ok;
+  s->hlld_hllc = c.hlld_hllc;
+  s->pcm_retry = c.pcm_retry;
+  return MGPU_OK;
+}
+
+int mgpu_measure_divB(mgpu_solver *h, double *mean, double *max)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (h->g.nd < 2) {
+    *mean = 0.0;
+    *max = 0.0;
+    return MGPU_OK;
+  }
+  if (fp32(h)) k_divB<float><<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, (const float *) h->b.PA, h->red);
+  else k_divB<double><<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, (const double *) h->b.PA, h->red);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->red_host, h->red, sizeof(double) * 2 * RED_BLOCKS, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  double sum = 0.0, mx = 0.0;   // zones outside the stencil's range count as div = 0
+  for (int b = 0; b < RED_BLOCKS; ++b) {
+    sum += h->red_host[2 * b];
+    mx = fmax(mx, h->red_host[2 * b + 1]);
+  }
+  long long glb = 1;
+  for (int d = 0; d < h->g.nd; ++d) glb *= h->N[d];
+  *mean = (sum / (double) h->g.nz) / (double) glb;
+  *max = mx;
+  return MGPU_OK;
+}
+
+int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (fp32(h)) k_wmax<float><<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, (const float *) h->b.PA, h->red);
+  else k_wmax<double><<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, (const double *) h->b.PA, h->red);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->red_host, h->red, sizeof(double) * RED_BLOCKS, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  double mx = 0.0;
+  for (int b = 0; b < RED_BLOCKS; ++b) mx = fmax(mx, h->red_host[b]);
+  *wmax = mx;
+  return MGPU_OK;
+}
+
+int mgpu_profile_enable(mgpu_solver *h, int capacity)
+{
+  if (!h || capacity <= 0) return MGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  prof_free(h);
+  h->prof_ev.resize(2 * (size_t) capacity);
+  for (auto &e : h->prof_ev) CK(cudaEventCreate(&e));
+  h->prof_tag.assign(capacity, 0);
+  h->prof_units.assign(capacity, 0);
+  h->prof_count = 0;
+  h->prof.ev = h->prof_ev.data();
+  h->prof.tag = h->prof_tag.data();
+  h->prof.units = h->prof_units.data();
+  h->prof.capacity = capacity;
+  h->prof.count = &h->prof_count;
+  h->prof_on = true;
+  return MGPU_OK;
+}
+
+int mgpu_profile_disable(mgpu_solver *h)
+{
+  if (!h) return MGPU_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  prof_free(h);
+  return MGPU_OK;
+}
+
+int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long *units)
+{
+  if (!h || !ms || !launches || !units) return MGPU_ERR_ARG;
+  if (!h->prof_on) return fail(h, MGPU_ERR_STATE, "profiling is not enabled");
+  CK(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < KC_COUNT; ++c) { ms[c] = 0.0; launches[c] = 0; units[c] = 0; }
+  for (int i = 0; i < h->prof_count; ++i) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]));
+    const int c = h->prof_tag[i];
+    ms[c] += t;
+    launches[c] += 1;
+    units[c] += h->prof_units[i];
+  }
+  h->prof_count = 0;
+  return MGPU_OK;
+}
+
+int mgpu_set_c2p_network(mgpu_solver *h, const float *params, long long count)
+{
+  if (!h || !params || count <= 0) return MGPU_ERR_ARG;
+  if (h->mlp) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->mlp);
+    h->mlp = nullptr;
+  }
+  CK(cudaMalloc((void **) &h->mlp, count * sizeof(float)));
+  CK(cudaMemcpy(h->mlp, params, count * sizeof(float), cudaMemcpyHostToDevice));
+  h->mlp_count = count;
+  return MGPU_OK;
+}
+
+}  // extern "C"

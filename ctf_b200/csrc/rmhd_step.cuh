@@ -1,0 +1,382 @@
+// Step kernels of the B200 RMHD advance, templated on the bulk type T.
+//
+// Data layout in HBM (structure of arrays, one contiguous array per component):
+//   zone index z = (i*G1 + j)*G2 + k over the guarded grid (x slowest, as in the reference's
+//   AoS layout, Mara/hydro.cpp:80-110), component c at base + c*cs.
+//   "state" arrays (committed prims, conserved RK registers): components 0..4 in T,
+//                 components 5..7 (the magnetic field) in double, always;
+//   "face" arrays (stage prims PA, fluxes F/G/H): all 8 components in T.
+// Guard zones of a state are never read: the c2p kernel writes each interior zone's
+// primitives to the zone and to every periodic image of it in the guard layers, which gives
+// exactly the arrays SimpleCartesianDomain::Synchronize (Mara/simple-cart.cpp:81-174) would.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "rmhd_physics.cuh"
+
+namespace mgpu {
+
+__device__ __forceinline__ bool stage_failed(const Ctl *ctl, int upto)
+{
+  int e = 0;
+  for (int s = 0; s < upto && s < MAX_STAGES; ++s) e |= ctl->stage_err[s];
+  return e != 0;
+}
+
+// Positions of zone m_d and its periodic guard images along one dimension.
+__device__ __forceinline__ int images_1d(int m, int n, int ng, bool active, int *pos)
+{
+  pos[0] = m;
+  if (!active) return 1;
+  int c = 1;
+  if (m - n >= 0 && m - n < ng) pos[c++] = m - n;
+  if (m + n >= n + ng && m + n < n + 2 * ng) pos[c++] = m + n;
+  return c;
+}
+
+__device__ __forceinline__ int multiplicity(const Grid &g, int i, int j, int k)
+{
+  int p[3];
+  return images_1d(i, g.n[0], g.ng, g.nd >= 1, p) * images_1d(j, g.n[1], g.ng, g.nd >= 2, p) *
+         images_1d(k, g.n[2], g.ng, g.nd >= 3, p);
+}
+
+template <class T>
+__device__ __forceinline__ void load_state(const Grid &g, StateCPtr<T> s, long long z, double *U)
+{
+#pragma unroll
+  for (int c = 0; c < 5; ++c) U[c] = double(s.bulk[c * g.cs + z]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) U[5 + c] = s.B[c * g.cs + z];
+}
+
+// Warp-aggregated counter increment.
+__device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned v)
+{
+  const unsigned mask = __activemask();
+  const unsigned sum = __reduce_add_sync(mask, v);
+  if ((threadIdx.x & 31) == __ffs(mask) - 1 && sum) atomicAdd(ctr, (unsigned long long) sum);
+}
+
+// ---- begin: dt and counters ----------------------------------------------------------------
+// dt_mode 0: dt given by the host; 1: dt = cfl * min_dx / MaxLambda of the previous advance
+// (luaC_Mara_get_timestep, Mara/mara.cpp:374-381), computed on the device.
+static __global__ void k_begin(Ctl *ctl, int dt_mode, double dt, double cfl, double min_dx)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (dt_mode == 1) dt = cfl * min_dx / __longlong_as_double((long long) ctl->max_lambda_bits);
+    ctl->dt = dt;
+    ctl->max_lambda_bits = 0ull;   // RiemannSolver::ResetMaxLambda
+    for (int s = 0; s < MAX_STAGES; ++s) ctl->stage_err[s] = 0;
+    ctl->final_err = 0;
+    ctl->committed = 0;
+    ctl->c2p_calls = ctl->c2p_iters = 0;
+    for (int a = 0; a < 6; ++a) ctl->c2p_attempt[a] = 0;
+    ctl->face_c2p_calls = ctl->face_c2p_iters = 0;
+    ctl->hlld_ok = ctl->hlld_hllc = ctl->pcm_retry = 0;
+  }
+}
+
+static __global__ void k_commit(Ctl *ctl, int nstages)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int e = 0;
+    for (int s = 0; s < nstages; ++s) e |= ctl->stage_err[s];
+    e |= ctl->final_err;
+    if (e == 0) {
+      ctl->cur ^= 1;
+      ctl->committed = 1;
+    }
+  }
+}
+
+// ---- P -> U on interior zones (GodunovOperator::PrimToCons, Mara/hydro.cpp:112-123) ----------
+template <class T>
+__global__ void __launch_bounds__(256) k_prim_to_cons(Grid g, StateCPtr<T> P0, StateCPtr<T> P1, StatePtr<T> U,
+                                                      double gamma, const Ctl *ctl)
+{
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  int i, j, k;
+  interior_coords(g, t, i, j, k);
+  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+  const StateCPtr<T> P = ctl->cur ? P1 : P0;
+  double p[8], u[8];
+  load_state(g, P, z, p);
+  prim_to_cons(gamma, p, u);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) U.bulk[c * g.cs + z] = T(u[c]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) U.B[c * g.cs + z] = u[5 + c];
+}
+
+// ---- c2p with guard scatter (GodunovOperator::ConsToPrim, Mara/hydro.cpp:125-202) -----------
+// Stage c2p (final == 0): guess from PA (or zeros on the first stage, as the reference's
+// PrimitiveArray is zero-filled by every advance, Mara/mara.cpp:321); result into PA.
+// Closing c2p (final == 1): guess from PA, result into the next committed state.
+template <class T>
+__global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
+                                                      PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
+                                                      int ereset, double preset, double dreset)
+{
+  if (stage_failed(ctl, stage)) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  int i, j, k;
+  interior_coords(g, t, i, j, k);
+  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+  double u[8], p[8];
+  load_state(g, U, z, u);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+  C2PTally tally;
+  int err = cons_to_prim(pp, u, p, &tally) != 0;
+  warp_add(&ctl->c2p_calls, 1u);
+  warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
+  if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
+  if (err) {
+    if (ereset) {   // emergency reset of the failed zone
+      p[0] = dreset;
+      p[1] = preset;
+      p[2] = p[3] = p[4] = 0.0;
+      p[5] = u[5];
+      p[6] = u[6];
+      p[7] = u[7];
+    } else {
+      atomicAdd(final ? &ctl->final_err : &ctl->stage_err[stage], multiplicity(g, i, j, k));
+    }
+  }
+  int pi[3], pj[3], pk[3];
+  const int ni = images_1d(i, g.n[0], g.ng, g.nd >= 1, pi);
+  const int nj = images_1d(j, g.n[1], g.ng, g.nd >= 2, pj);
+  const int nk = images_1d(k, g.n[2], g.ng, g.nd >= 3, pk);
+  StatePtr<T> Pn = ctl->cur ? Pn0 : Pn1;   // the buffer that is not committed
+  for (int a = 0; a < ni; ++a)
+    for (int b = 0; b < nj; ++b)
+      for (int c = 0; c < nk; ++c) {
+        const long long w = ((long long) pi[a] * g.G[1] + pj[b]) * g.G[2] + pk[c];
+        if (final) {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) Pn.bulk[q * g.cs + w] = T(p[q]);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) Pn.B[q * g.cs + w] = p[5 + q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) PA[q * g.cs + w] = T(p[q]);
+        }
+      }
+}
+
+// ---- flux sweep (MethodOfLinesSplit::intercell_flux_sweep, Mara/plm-split.cpp:43-73) ---------
+// One thread per face.  The face set is the reference's: every zone index f with
+// 2*S <= f < nz - 3*S in the flattened guarded array (S the zone stride of `dim`), the face
+// between zones f and f + S.  Faces that straddle a row end in the flattened array are
+// evaluated too, because they enter MaxLambda in the reference.
+template <class T>
+__global__ void __launch_bounds__(128) k_flux(Grid g, int dim, const T *__restrict__ PA, T *__restrict__ F,
+                                              PhysParams pp, Ctl *ctl, int stage)
+{
+  if (stage_failed(ctl, stage + 1)) return;
+  const long long S = g.s[dim - 1];
+  const long long f = 2 * S + (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  T ml = T(0);
+  int used_hllc = 0, pcm_retry = 0, hlld = 0;
+  C2PTally tally{0, 0};
+  if (f < g.nz - 3 * S) {
+    T Pl[8], Pr[8];
+    const T theta = T(pp.theta);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const T *a = PA + q * g.cs + f;
+      if (pp.recon == RECON_PCM) {
+        Pl[q] = a[0];
+        Pr[q] = a[S];
+      } else if (pp.recon == RECON_PLM) {
+        const T vm = a[-S], v0 = a[0], vp = a[S], vpp = a[2 * S];
+        Pl[q] = plm(theta, vm, v0, vp, T(+1));
+        Pr[q] = plm(theta, v0, vp, vpp, T(-1));
+      } else {
+        const T vm2 = a[-2 * S], vm1 = a[-S], v0 = a[0], vp1 = a[S], vp2 = a[2 * S], vp3 = a[3 * S];
+        Pl[q] = weno5(pp.is_mode, T(pp.sz10A), vm2, vm1, v0, vp1, vp2, true);
+        Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
+      }
+    }
+    T Fo[8];
+    const T gamma = T(pp.gamma);
+    int err;
+    if (pp.riemann == RIEMANN_HLLD) {
+      hlld = 1;
+      err = riemann_hlld<T>(pp, Pl, Pr, Fo, dim, ml, used_hllc, &tally);
+    } else if (pp.riemann == RIEMANN_HLLC) {
+      err = riemann_hllc<T>(gamma, Pl, Pr, Fo, dim, ml);
+    } else {
+      err = riemann_hll<T>(gamma, Pl, Pr, Fo, dim, ml);
+    }
+    if (err) {   // retry with the zone states themselves (PCM)
+      pcm_retry = 1;
+      T tally_iters = 0;
+      (void) tally_iters;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        Pl[q] = PA[q * g.cs + f];
+        Pr[q] = PA[q * g.cs + f + S];
+      }
+      C2PTally t2{0, 0};
+      if (pp.riemann == RIEMANN_HLLD) err = riemann_hlld<T>(pp, Pl, Pr, Fo, dim, ml, used_hllc, &t2);
+      else if (pp.riemann == RIEMANN_HLLC) err = riemann_hllc<T>(gamma, Pl, Pr, Fo, dim, ml);
+      else err = riemann_hll<T>(gamma, Pl, Pr, Fo, dim, ml);
+      tally.iters += t2.iters;
+      tally.attempts += t2.attempts;
+      if (err) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) Fo[q] = T(0);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
+  }
+  // MaxLambda: warp max -> block max -> one atomic per block (non-negative doubles order
+  // like their bit patterns)
+  double m = double(ml);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double wmax[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wmax[warp] = m;
+  __syncthreads();
+  if (warp == 0) {
+    m = lane < (blockDim.x >> 5) ? wmax[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0 && m > 0.0) atomicMax(&ctl->max_lambda_bits, (unsigned long long) __double_as_longlong(m));
+  }
+  if (hlld) {
+    warp_add(&ctl->hlld_ok, (unsigned) (1 - used_hllc));
+    warp_add(&ctl->hlld_hllc, (unsigned) used_hllc);
+  }
+  warp_add(&ctl->pcm_retry, (unsigned) pcm_retry);
+  warp_add(&ctl->face_c2p_calls, (unsigned) (tally.attempts > 0));
+  warp_add(&ctl->face_c2p_iters, (unsigned) tally.iters);
+}
+
+// ---- CT + flux divergence + Runge-Kutta combine ---------------------------------------------
+// Flux-CT (AdiabaticIdealRmhd::ConstrainedTransport3d/2d, Mara/rmhd.cpp:311-381), the
+// divergence L = -(dF/dx + dG/dy + dH/dz) (Mara/plm-split.cpp:75-122) and the stage combine
+// of Mara/runge-kutta.hpp:129-177, fused, on interior zones only.
+struct UpdateArgs {
+  int combine;
+  double c;        // COMB_RK4_K coefficient
+};
+
+template <class T>
+__device__ __forceinline__ double fval(const T *F, const Grid &g, int q, long long z)
+{
+  return double(F[q * g.cs + z]);
+}
+
+// 8-point corner-EMF average for the B-flux component (normal dir a, field component b):
+// (2 F0 + F[+b] + F[-b] - G0 - G[+a] - G[-b] - G[+a-b]) / 8 with F the a-flux of B_b and G
+// the b-flux of B_a, strides sa (normal dir) and sb (field dir).
+template <class T>
+__device__ __forceinline__ double ct_emf(const T *Fa, const T *Fb, const Grid &g, int qb, int qa, long long z,
+                                         long long sa, long long sb)
+{
+  const T *F = Fa + qb * g.cs + z;
+  const T *G = Fb + qa * g.cs + z;
+  return (2 * double(F[0]) + double(F[sb]) + double(F[-sb]) - double(G[0]) - double(G[sa]) - double(G[-sb]) -
+          double(G[sa - sb])) * 0.125;
+}
+
+template <class T>
+__device__ __forceinline__ T combine_bulk(const UpdateArgs &a, T un, T us, T dt, T L, T *K, T k1, T k2, T k3)
+{
+  switch (a.combine) {
+  case COMB_EULER: return un + dt * L;
+  case COMB_RK2_2: return T(0.5) * (un + us + dt * L);
+  case COMB_RK3_2: return T(3. / 4) * un + T(1. / 4) * us + T(1. / 4) * dt * L;
+  case COMB_RK3_3: return T(1. / 3) * un + T(2. / 3) * us + T(2. / 3) * dt * L;
+  case COMB_RK4_K: { const T kk = dt * L; *K = kk; return un + T(a.c) * kk; }
+  default: return un + (T(1.0) / T(6.0)) * (k1 + T(2.0) * k2 + T(2.0) * k3 + dt * L);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
+                                                const T *__restrict__ F, const T *__restrict__ G,
+                                                const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
+                                                StateCPtr<T> K1, StateCPtr<T> K2, StateCPtr<T> K3,
+                                                const Ctl *ctl, int stage)
+{
+  if (stage_failed(ctl, stage + 1)) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  int i, j, k;
+  interior_coords(g, t, i, j, k);
+  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+  const long long sx = g.s[0], sy = g.s[1], sz = g.s[2];
+  const double dx = g.dx, dy = g.dy, dz = g.dz;
+  const double dtd = ctl->dt;
+  const T dt = T(dtd);
+  const bool rk4 = a.combine >= COMB_RK4_K;
+  // bulk components 0..4: plain flux differences in T
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    T L;
+    if (g.nd == 1) {
+      L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx);
+    } else if (g.nd == 2) {
+      L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx) - (G[q * g.cs + z] - G[q * g.cs + z - sy]) / T(dy);
+    } else {
+      L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx) - (G[q * g.cs + z] - G[q * g.cs + z - sy]) / T(dy) -
+          (H[q * g.cs + z] - H[q * g.cs + z - sz]) / T(dz);
+    }
+    const T un = Un.bulk[q * g.cs + z];
+    const T us = (a.combine == COMB_RK2_2 || a.combine == COMB_RK3_2 || a.combine == COMB_RK3_3) ? Us.bulk[q * g.cs + z] : T(0);
+    T k1 = T(0), k2 = T(0), k3 = T(0), kk = T(0);
+    if (a.combine == COMB_RK4_4) { k1 = K1.bulk[q * g.cs + z]; k2 = K2.bulk[q * g.cs + z]; k3 = K3.bulk[q * g.cs + z]; }
+    Uout.bulk[q * g.cs + z] = combine_bulk<T>(a, un, us, dt, L, &kk, k1, k2, k3);
+    if (rk4 && a.combine == COMB_RK4_K) Kout.bulk[q * g.cs + z] = kk;
+  }
+  // magnetic components 5..7 in double, with the constrained-transport fluxes
+  double Lb[3];
+  if (g.nd == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Lb[c] = -(fval(F, g, 5 + c, z) - fval(F, g, 5 + c, z - sx)) / dx;
+  } else if (g.nd == 2) {
+    // CT2d: Fx[Bx] = 0, Fx[By] = FxBy, Fy[Bx] = FyBx, Fy[By] = 0; Bz keeps its Godunov fluxes
+    const double FxBy0 = ct_emf(F, G, g, By, Bx, z, sx, sy), FxBym = ct_emf(F, G, g, By, Bx, z - sx, sx, sy);
+    const double FyBx0 = ct_emf(G, F, g, Bx, By, z, sy, sx), FyBxm = ct_emf(G, F, g, Bx, By, z - sy, sy, sx);
+    Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy;
+    Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy;
+    Lb[2] = -(fval(F, g, Bz, z) - fval(F, g, Bz, z - sx)) / dx - (fval(G, g, Bz, z) - fval(G, g, Bz, z - sy)) / dy;
+  } else {
+    const double FxBy0 = ct_emf(F, G, g, By, Bx, z, sx, sy), FxBym = ct_emf(F, G, g, By, Bx, z - sx, sx, sy);
+    const double FyBx0 = ct_emf(G, F, g, Bx, By, z, sy, sx), FyBxm = ct_emf(G, F, g, Bx, By, z - sy, sy, sx);
+    const double FyBz0 = ct_emf(G, H, g, Bz, By, z, sy, sz), FyBzm = ct_emf(G, H, g, Bz, By, z - sy, sy, sz);
+    const double FzBy0 = ct_emf(H, G, g, By, Bz, z, sz, sy), FzBym = ct_emf(H, G, g, By, Bz, z - sz, sz, sy);
+    const double FzBx0 = ct_emf(H, F, g, Bx, Bz, z, sz, sx), FzBxm = ct_emf(H, F, g, Bx, Bz, z - sz, sz, sx);
+    const double FxBz0 = ct_emf(F, H, g, Bz, Bx, z, sx, sz), FxBzm = ct_emf(F, H, g, Bz, Bx, z - sx, sx, sz);
+    Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy - (FzBx0 - FzBxm) / dz;
+    Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy - (FzBy0 - FzBym) / dz;
+    Lb[2] = -(FxBz0 - FxBzm) / dx - (FyBz0 - FyBzm) / dy - (0.0 - 0.0) / dz;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double un = Un.B[c * g.cs + z];
+    const double L = Lb[c];
+    double out;
+    switch (a.combine) {
+    case COMB_EULER: out = un + dtd * L; break;
+    case COMB_RK2_2: out = 0.5 * (un + Us.B[c * g.cs + z] + dtd * L); break;
+    case COMB_RK3_2: out = 3. / 4 * un + 1. / 4 * Us.B[c * g.cs + z] + 1. / 4 * dtd * L; break;
+    case COMB_RK3_3: out = 1. / 3 * un + 2. / 3 * Us.B[c * g.cs + z] + 2. / 3 * dtd * L; break;
+    case COMB_RK4_K: { const double kk = dtd * L; Kout.B[c * g.cs + z] = kk; out = un + a.c * kk; } break;
+    default:
+      out = un + (1.0 / 6.0) * (K1.B[c * g.cs + z] + 2.0 * K2.B[c * g.cs + z] + 2.0 * K3.B[c * g.cs + z] + dtd * L);
+      break;
+    }
+    Uout.B[c * g.cs + z] = out;
+  }
+}
+
+}  // namespace mgpu

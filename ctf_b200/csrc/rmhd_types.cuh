@@ -1,0 +1,160 @@
+// Plain data shared by the host library and the kernel translation units: physics
+// parameters, the grid description, the device control block and the launch arguments.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mgpu {
+
+enum { ddd = 0, tau = 1, Sx = 2, Sy = 3, Sz = 4, Bx = 5, By = 6, Bz = 7 };   // conserved
+enum { rho = 0, pre = 1, vx = 2, vy = 3, vz = 4 };                            // primitive
+
+enum C2PError {
+  C2P_SUCCESS = 0, C2P_CONS_NAN, C2P_CONS_NEG_DENSITY, C2P_CONS_NEG_ENERGY, C2P_PRIM_NAN,
+  C2P_PRIM_NEG_PRESSURE, C2P_PRIM_NEG_RESTMASS, C2P_PRIM_SUPERLUMINAL, C2P_MAXITER
+};
+
+enum Recon { RECON_PCM = 0, RECON_PLM = 1, RECON_WENO5 = 2 };
+enum Riemann { RIEMANN_HLL = 0, RIEMANN_HLLC = 1, RIEMANN_HLLD = 2 };
+enum ISMode { IS_JS96 = 0, IS_B08 = 1, IS_SZ10 = 2 };
+
+// Solver constants that enter the physics (mirrors of the reference's global statics).
+struct PhysParams {
+  double gamma;      // AdiabaticEos::Gamma
+  double pfloor;     // rmhd_c2p_set_pressure_floor
+  double theta;      // reconstruct_set_plm_theta
+  double sz10A;      // reconstruct_set_shenzha10_A
+  int is_mode;       // reconstruct_set_smoothness_indicator
+  int recon;         // GodunovOperator::reconstruct_method
+  int riemann;
+  int learned;       // learned c2p initial guess on/off
+  const void *mlp;   // device pointer to the packed c2p network (nullptr when off)
+};
+
+constexpr int MAX_STAGES = 4;
+
+// Device control block of one solver (one per handle, in device memory).
+struct Ctl {
+  unsigned long long max_lambda_bits;   // MaxLambda of the current/last advance (double bits)
+  double dt;                            // dt used by the current/last advance
+  int stage_err[MAX_STAGES];            // c2p failures per stage (guard images included)
+  int final_err;                        // failures of the closing c2p
+  int cur;                              // committed primitive buffer (0/1)
+  int committed;                        // 1 if the last advance was committed
+  int pad;
+  // statistics, accumulated over the advance
+  unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
+  unsigned long long face_c2p_calls, face_c2p_iters;
+  unsigned long long hlld_ok, hlld_hllc, pcm_retry;
+};
+
+struct Grid {
+  int nd, ng;
+  int n[3];       // interior zones per dim (1 for unused dims)
+  int G[3];       // guarded extent per dim (1 for unused dims)
+  long long nz;   // guarded zones
+  long long cs;   // component stride of the SoA arrays (elements)
+  long long s[3]; // zone strides of x, y, z
+  double dx, dy, dz;
+  long long ninterior;
+};
+
+template <class T> struct StatePtr {   // components 0..4 in T, 5..7 in double
+  T *bulk;
+  double *B;
+};
+template <class T> struct StateCPtr {
+  const T *bulk;
+  const double *B;
+};
+
+__device__ __forceinline__ void interior_coords(const Grid &g, long long t, int &i, int &j, int &k)
+{
+  const long long nyz = (long long) g.n[1] * g.n[2];
+  i = (int) (t / nyz);
+  const long long r = t - (long long) i * nyz;
+  j = (int) (r / g.n[2]);
+  k = (int) (r - (long long) j * g.n[2]);
+  i += g.ng;
+  if (g.nd >= 2) j += g.ng;
+  if (g.nd >= 3) k += g.ng;
+}
+
+struct AdvanceBuffers {
+  void *Pc_bulk[2];
+  double *Pc_B[2];
+  void *PA;
+  void *U0_bulk, *U1_bulk, *K_bulk[3];
+  double *U0_B, *U1_B, *K_B[3];
+  void *F[3];
+};
+
+// Optional per-launch timing: the launcher records an event pair around every kernel and
+// tags it with its class (KC_*); the host sums the elapsed times after a synchronize.
+enum KernelClass { KC_BEGIN = 0, KC_P2C = 1, KC_C2P = 2, KC_FLUX = 3, KC_UPDATE = 4, KC_COUNT = 5 };
+struct LaunchProfiler {
+  cudaEvent_t *ev;    // 2 * capacity events
+  int *tag;
+  long long *units;   // work units of the launch (faces or zones)
+  int capacity;
+  int *count;         // host counter
+};
+
+struct AdvanceArgs {
+  Grid g;
+  PhysParams pp;
+  int rk;           // 1 single, 2 rk2, 3 rk3, 4 rk4
+  int ereset;
+  double preset, dreset;
+  int dt_mode;      // 0: dt from the host, 1: dt = cfl*min_dx/MaxLambda(previous)
+  double dt, cfl, min_dx;
+  AdvanceBuffers b;
+  Ctl *ctl;
+  cudaStream_t stream;
+  LaunchProfiler *prof;   // nullptr: no timing
+};
+
+enum Combine {
+  COMB_EULER = 0,     // Uout = Un + dt L                        (single; RK2/RK3 stage 1)
+  COMB_RK2_2 = 1,     // Uout = 0.5 (Un + Us + dt L)
+  COMB_RK3_2 = 2,     // Uout = 3/4 Un + 1/4 Us + 1/4 dt L
+  COMB_RK3_3 = 3,     // Uout = 1/3 Un + 2/3 Us + 2/3 dt L
+  COMB_RK4_K = 4,     // K = dt L; Uout = Un + c K                (c = 1/2, 1/2, 1)
+  COMB_RK4_4 = 5      // Uout = Un + 1/6 (K1 + 2 K2 + 2 K3 + dt L)
+};
+
+struct StageKind {
+  int combine;
+  double c;
+};
+
+inline int num_stages(int rk) { return rk == 1 ? 1 : rk == 2 ? 2 : rk == 3 ? 3 : 4; }
+
+inline StageKind stage_kind(int rk, int s)
+{
+  switch (rk) {
+  case 1: return {COMB_EULER, 0};
+  case 2: return {s == 0 ? COMB_EULER : COMB_RK2_2, 0};
+  case 3: return {s == 0 ? COMB_EULER : s == 1 ? COMB_RK3_2 : COMB_RK3_3, 0};
+  default: return {s == 3 ? COMB_RK4_4 : COMB_RK4_K, s == 2 ? 1.0 : 0.5};
+  }
+}
+
+struct TransferArgs {
+  Grid g;
+  AdvanceBuffers b;
+  Ctl *ctl;
+  cudaStream_t stream;
+};
+
+}  // namespace mgpu
+
+// Entry points exported by each precision's translation unit.
+#define MGPU_DECLARE_PRECISION(suffix)                                                                   \
+  namespace mgpu {                                                                                       \
+  cudaError_t advance_##suffix(const AdvanceArgs &A);                                                    \
+  cudaError_t upload_##suffix(const TransferArgs &A, const double *d_aos, long long z0, long long count); \
+  cudaError_t download_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count);     \
+  cudaError_t face_io_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count, int to_aos); \
+  }
+

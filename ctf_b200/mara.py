@@ -1,0 +1,404 @@
+"""Host-side mirror of the reference's Lua module ``Mara`` over the B200 C ABI.
+
+The reference's drivers (``modules/MaraSim.lua``, ``ctf-core/run-mara.lua``) call::
+
+    Mara.start(); Mara.set_fluid('rmhd'); Mara.set_eos('gamma-law', 4/3)
+    Mara.set_boundary('periodic'); Mara.set_riemann('hlld'); Mara.set_godunov('plm-split')
+    Mara.set_advance('rk2'); Mara.config_solver{extrap='plm', theta=2.0}
+    Mara.set_domain({0,0,0}, {1,1,1}, {N,N,N}, 8, 3)
+    local kzps, errors = Mara.advance(P, dt);  local dt = Mara.get_timestep(0.3)
+
+The same calls, with the same argument meaning, names and error behaviour (misuse raises
+:class:`MaraError`, the analogue of ``luaL_error``; numerical failure is a returned error
+count with the state left unchanged), work on :data:`Mara` here, with the step running on
+the GPU (``Mara/mara.cpp:137-1167`` is the surface mirrored).  ``P`` is a float64 numpy
+array in the reference's AoS layout with guard zones, shape ``(G0, G1, G2, 8)``.
+
+:class:`Solver` is the object-level API under it: one handle, device-resident state.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+RECON = {"pcm": 0, "plm": 1, "weno5": 2}
+RIEMANN = {"hll": 0, "hllc": 1, "hlld": 2}
+ADVANCE = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}
+IS_MODE = {"js96": 0, "b08": 1, "sz10": 2}
+PRECISION = {"fp64": 0, "fp32": 1}
+PRIM_NAMES = ["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]   # Mara/rmhd.cpp:72-78
+
+
+class MaraError(RuntimeError):
+    """API misuse (the reference raises luaL_error in these cases)."""
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclass
+class Scheme:
+    """Solver selection (the union of the reference's set_* selectors and config_solver)."""
+    gamma: float = 4.0 / 3.0
+    extrap: str = "plm"
+    theta: float = 2.0
+    IS: str = "js96"
+    sz10A: float = 50.0
+    riemann: str = "hlld"
+    advance: str = "rk2"
+    pfloor: float = -1.0
+    ereset: bool = False
+    preset: float = 1.0
+    dreset: float = 1.0
+    precision: str = "fp64"
+    learned_c2p: bool = False
+
+    def to_config(self) -> _lib.MgpuConfig:
+        lib = _lib.load()
+        c = _lib.MgpuConfig()
+        lib.mgpu_default_config(ctypes.byref(c))
+        c.gamma = self.gamma
+        c.recon = RECON[self.extrap]
+        c.theta = self.theta
+        c.is_mode = IS_MODE[self.IS]
+        c.sz10A = self.sz10A
+        c.riemann = RIEMANN[self.riemann]
+        c.rk = ADVANCE[self.advance]
+        c.pfloor = self.pfloor
+        c.ereset = int(self.ereset)
+        c.preset = self.preset
+        c.dreset = self.dreset
+        c.precision = PRECISION[self.precision]
+        c.learned_c2p = int(self.learned_c2p)
+        return c
+
+
+class Solver:
+    """One GPU solver handle with a device-resident primitive state."""
+
+    def __init__(self, scheme: Scheme, n, x0=None, x1=None, ng: int = 3, stream=None):
+        self.lib = _lib.load()
+        self.scheme = scheme
+        h = ctypes.c_void_p()
+        cfg = scheme.to_config()
+        rc = self.lib.mgpu_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc:
+            raise MaraError(f"mgpu_create failed ({rc})")
+        self.h = h
+        if stream is not None:
+            self._check(self.lib.mgpu_set_stream(self.h, ctypes.c_void_p(stream)))
+        n = tuple(int(v) for v in n)
+        nd = len(n)
+        x0 = tuple(x0) if x0 is not None else (0.0,) * nd
+        x1 = tuple(x1) if x1 is not None else (1.0,) * nd
+        self.n, self.nd, self.ng = n, nd, ng
+        self.shape = tuple(v + 2 * ng for v in n) + (1,) * (3 - nd) + (8,)
+        arr_x0 = (ctypes.c_double * nd)(*x0)
+        arr_x1 = (ctypes.c_double * nd)(*x1)
+        arr_n = (ctypes.c_int * nd)(*n)
+        self._check(self.lib.mgpu_set_domain(self.h, arr_x0, arr_x1, arr_n, nd, 8, ng))
+
+    def _check(self, rc):
+        if rc:
+            raise MaraError(f"[Mara] {self.lib.mgpu_last_error(self.h).decode()} (code {rc})")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_zones(self) -> int:
+        nz = ctypes.c_longlong()
+        self._check(self.lib.mgpu_num_zones(self.h, ctypes.byref(nz)))
+        return nz.value
+
+    def _check_buf(self, P):
+        if not (isinstance(P, np.ndarray) and P.dtype == np.float64 and P.flags.c_contiguous):
+            raise MaraError("[Mara] primitive must be a C-contiguous float64 array")
+        if P.size != self.num_zones * 8:
+            raise MaraError("[Mara] primitive has the wrong size for the domain")
+
+    def upload(self, P: np.ndarray):
+        self._check_buf(P)
+        self._check(self.lib.mgpu_upload_prim(self.h, _dp(P)))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape)
+        self._check_buf(out)
+        self._check(self.lib.mgpu_download_prim(self.h, _dp(out)))
+        return out
+
+    def upload_device(self, ptr: int):
+        self._check(self.lib.mgpu_upload_prim_device(self.h, ctypes.c_void_p(ptr)))
+
+    def download_device(self, ptr: int):
+        self._check(self.lib.mgpu_download_prim_device(self.h, ctypes.c_void_p(ptr)))
+
+    def advance(self, dt: float) -> int:
+        e = ctypes.c_int()
+        self._check(self.lib.mgpu_advance(self.h, ctypes.c_double(dt), ctypes.byref(e)))
+        return e.value
+
+    def advance_host(self, P: np.ndarray, dt: float):
+        self._check_buf(P)
+        kz, e = ctypes.c_double(), ctypes.c_int()
+        self._check(self.lib.mgpu_advance_host(self.h, _dp(P), ctypes.c_double(dt), ctypes.byref(kz),
+                                               ctypes.byref(e)))
+        return kz.value, e.value
+
+    def advance_async(self, n: int, dt: float | None = None, cfl: float = 0.3):
+        mode = 0 if dt is not None else 1
+        self._check(self.lib.mgpu_advance_async(self.h, int(n), mode, ctypes.c_double(dt or 0.0),
+                                                ctypes.c_double(cfl)))
+
+    def synchronize(self):
+        self._check(self.lib.mgpu_synchronize(self.h))
+
+    def get_timestep(self, cfl: float) -> float:
+        dt = ctypes.c_double()
+        self._check(self.lib.mgpu_get_timestep(self.h, ctypes.c_double(cfl), ctypes.byref(dt)))
+        return dt.value
+
+    def stats(self) -> dict:
+        s = _lib.MgpuStats()
+        self._check(self.lib.mgpu_get_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    @property
+    def max_lambda(self) -> float:
+        return self.stats()["max_lambda"]
+
+    def set_primitive(self, P: np.ndarray):
+        self._check_buf(P)
+        self._check(self.lib.mgpu_set_primitive(self.h, _dp(P)))
+
+    def mean_max_divB(self):
+        m, x = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mgpu_measure_divB(self.h, ctypes.byref(m), ctypes.byref(x)))
+        return m.value, x.value
+
+    def max_lorentz_factor(self) -> float:
+        w = ctypes.c_double()
+        self._check(self.lib.mgpu_max_lorentz_factor(self.h, ctypes.byref(w)))
+        return w.value
+
+    KERNEL_CLASSES = ["begin", "p2c", "c2p", "flux", "update"]
+
+    def profile_enable(self, capacity: int = 4096):
+        self._check(self.lib.mgpu_profile_enable(self.h, int(capacity)))
+
+    def profile_disable(self):
+        self._check(self.lib.mgpu_profile_disable(self.h))
+
+    def profile_read(self) -> dict:
+        """Per kernel class: summed ms, launches and work units since the last read."""
+        ms = (ctypes.c_double * 5)()
+        ln = (ctypes.c_longlong * 5)()
+        un = (ctypes.c_longlong * 5)()
+        self._check(self.lib.mgpu_profile_read(self.h, ms, ln, un))
+        return {k: {"ms": ms[i], "launches": ln[i], "units": un[i]}
+                for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def set_c2p_network(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.mgpu_set_c2p_network(
+            self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size))
+
+
+class _Measure:
+    def __init__(self, mod):
+        self._m = mod
+
+    def mean_max_divB(self):
+        return self._m._solver().mean_max_divB()
+
+    def max_lorentz_factor(self):
+        return self._m._solver().max_lorentz_factor()
+
+
+class _Fluid:
+    def __init__(self, mod):
+        self._m = mod
+
+    def GetPrimNames(self):
+        if self._m._fluid is None:
+            raise MaraError("[Mara] need a fluid to run this, use set_fluid")
+        return list(PRIM_NAMES)
+
+
+class MaraModule:
+    """The ``Mara`` table of the reference (Mara/mara.cpp:137-268), GPU-backed."""
+
+    def __init__(self):
+        self._reset()
+        self.measure = _Measure(self)
+        self.fluid = _Fluid(self)
+
+    def _reset(self):
+        self._scheme = Scheme()
+        self._fluid = None
+        self._boundary = None
+        self._godunov = None
+        self._domain = None
+        self._s = None
+        self._started = False
+
+    # lifecycle ---------------------------------------------------------------------------
+    def start(self):
+        """luaC_Mara_start (Mara/mara.cpp:271-287): a fresh application with defaults."""
+        self.close()
+        self._reset()
+        self._started = True
+
+    def close(self):
+        if self._s is not None:
+            self._s.close()
+        self._s = None
+
+    def _need_start(self):
+        if not self._started:
+            raise MaraError("[Mara] call Mara.start() first")
+
+    def _invalidate(self):
+        if self._s is not None:
+            self._s.close()
+            self._s = None
+
+    # selectors (Mara/mara.cpp:813-984, 1140-1167) ----------------------------------------
+    def set_fluid(self, key: str):
+        self._need_start()
+        if key != "rmhd":
+            raise MaraError(f"[Mara] no such fluid '{key}'" if key not in ("euler", "srhd")
+                            else f"[Mara] fluid '{key}' is not provided by the B200 module")
+        self._fluid = key
+        self._invalidate()
+
+    def set_eos(self, key: str, gamma: float = 1.4):
+        self._need_start()
+        if key != "gamma-law":
+            raise MaraError(f"[Mara] no such eos '{key}'")
+        self._scheme.gamma = float(gamma)
+        self._invalidate()
+
+    def set_boundary(self, key: str):
+        self._need_start()
+        if key != "periodic":
+            raise MaraError(f"[Mara] no such boundary conditions '{key}'")
+        self._boundary = key
+
+    def set_riemann(self, key: str):
+        self._need_start()
+        if key not in RIEMANN:
+            raise MaraError(f"[Mara] no such riemann solver '{key}'")
+        self._scheme.riemann = key
+        self._invalidate()
+
+    def set_godunov(self, key: str):
+        self._need_start()
+        if key != "plm-split":
+            raise MaraError(f"[Mara] no such integration scheme '{key}'")
+        self._godunov = key
+
+    def set_advance(self, key: str):
+        self._need_start()
+        if key not in ADVANCE:
+            raise MaraError(f"[Mara] no such advance option '{key}'")
+        self._scheme.advance = key
+        self._invalidate()
+
+    def config_solver(self, tbl: dict, quiet: bool = False):
+        """luaC_config_solver (Mara/mara.cpp:996-1138); also accepts precision/learned_c2p."""
+        self._need_start()
+        s = self._scheme
+        if "extrap" in tbl:
+            if tbl["extrap"] not in RECON:
+                raise MaraError(f"[Mara] no such extrap '{tbl['extrap']}'")
+            s.extrap = tbl["extrap"]
+        if "theta" in tbl:
+            s.theta = float(tbl["theta"])
+        if "IS" in tbl:
+            if tbl["IS"] not in IS_MODE:
+                raise MaraError(f"no such IS: {tbl['IS']}")
+            s.IS = tbl["IS"]
+        if "sz10A" in tbl:
+            s.sz10A = float(tbl["sz10A"])
+        if "pfloor" in tbl:
+            s.pfloor = float(tbl["pfloor"])
+        if "ereset" in tbl:
+            s.ereset = bool(tbl["ereset"])
+        if "preset" in tbl:
+            s.preset = float(tbl["preset"])
+        if "dreset" in tbl:
+            s.dreset = float(tbl["dreset"])
+        if "precision" in tbl:
+            if tbl["precision"] not in PRECISION:
+                raise MaraError(f"[Mara] no such precision '{tbl['precision']}'")
+            s.precision = tbl["precision"]
+        if "learned_c2p" in tbl:
+            s.learned_c2p = bool(tbl["learned_c2p"])
+        if not quiet:
+            for k, v in tbl.items():
+                print(f"[config] setting {k}={v}")
+        self._invalidate()
+
+    def set_domain(self, x0, x1, N, Nq: int = 8, Ng: int = 3):
+        """luaC_set_domain (Mara/mara.cpp:726-755)."""
+        self._need_start()
+        if Nq != 8:
+            raise MaraError("[Mara] the rmhd fluid has Nq = 8")
+        self._domain = (tuple(x0), tuple(x1), tuple(int(v) for v in N), int(Ng))
+        self._invalidate()
+
+    def _solver(self) -> Solver:
+        if self._domain is None:
+            raise MaraError("[Mara] need a domain to run this, use set_domain")
+        if self._s is None:
+            x0, x1, N, Ng = self._domain
+            self._s = Solver(self._scheme, N, x0, x1, Ng)
+        return self._s
+
+    # state -------------------------------------------------------------------------------
+    def init_prim(self, P: np.ndarray, f):
+        """luaC_Mara_init_prim (Mara/mara.cpp:531-632): P[zone] = f(x, y, z) on interior zones."""
+        s = self._solver()
+        s._check_buf(P)
+        x0, x1, N, Ng = self._domain
+        nd = len(N)
+        dx = [(x1[d] - x0[d]) / N[d] for d in range(nd)]
+        G = s.shape
+        it = [range(N[d]) for d in range(nd)]
+        import itertools
+        for idx in itertools.product(*it):
+            pos = [x0[d] + dx[d] * (idx[d] + 0.5) for d in range(nd)] + [0.0] * (3 - nd)
+            m = tuple(i + Ng for i in idx) + (0,) * (3 - nd)
+            P[m] = f(*pos)
+        del G
+        s.set_primitive(P)
+
+    def set_primitive(self, P: np.ndarray):
+        self._solver().set_primitive(P)
+
+    def advance(self, P: np.ndarray, dt: float):
+        """luaC_Mara_advance (Mara/mara.cpp:297-341): returns (kzps, errors); P is updated in
+        place only when errors == 0.  kzps counts guard zones, like the reference."""
+        return self._solver().advance_host(P, dt)
+
+    def get_timestep(self, cfl: float) -> float:
+        return self._solver().get_timestep(cfl)
+
+
+Mara = MaraModule()

@@ -1,0 +1,133 @@
+/* mara_gpu.h -- C ABI of the B200 RMHD step (libmaragpu.so).
+ *
+ * A drop-in for the CPU advance behind the reference's Lua module `Mara`
+ * (Mara/mara.cpp:137-268, registered by ctf-core/ctf.c:139).  Plain C types only: host
+ * pointers, device pointers as void*, sizes, int status codes (0 = ok, never an exception
+ * or longjmp across the boundary).  One handle = one solver = one CUDA stream; calls on one
+ * handle are not thread-safe, separate handles are independent (unlike the reference, whose
+ * solver is a process-global singleton, Mara/mara.cpp:135).
+ *
+ * Layout at the boundary is the reference's: AoS float64 primitives with guard zones,
+ * ((i*G1 + j)*G2 + k)*8 + q, q = rho, pre, vx, vy, vz, Bx, By, Bz (Mara/rmhd.hpp:20),
+ * G_d = N_d + 2*Ng.
+ */
+#ifndef MARA_GPU_H
+#define MARA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mgpu_solver mgpu_solver;
+
+enum { MGPU_OK = 0, MGPU_ERR_ARG = 1, MGPU_ERR_STATE = 2, MGPU_ERR_CUDA = 3, MGPU_ERR_NOMEM = 4,
+       MGPU_ERR_UNSUPPORTED = 5 };
+
+enum { MGPU_FLUID_RMHD = 0 };
+enum { MGPU_RECON_PCM = 0, MGPU_RECON_PLM = 1, MGPU_RECON_WENO5 = 2 };
+enum { MGPU_RIEMANN_HLL = 0, MGPU_RIEMANN_HLLC = 1, MGPU_RIEMANN_HLLD = 2 };
+enum { MGPU_IS_JS96 = 0, MGPU_IS_B08 = 1, MGPU_IS_SZ10 = 2 };
+enum { MGPU_PREC_FP64 = 0, MGPU_PREC_FP32 = 1 };
+
+/* Solver selection: the union of Mara.set_fluid/set_eos/set_godunov/set_riemann/set_advance
+ * and the keys of Mara.config_solver (Mara/mara.cpp:813-1167). */
+typedef struct {
+  int    fluid;        /* MGPU_FLUID_RMHD (set_fluid('rmhd')) */
+  double gamma;        /* set_eos('gamma-law', gamma) */
+  int    recon;        /* config_solver{extrap = 'pcm' | 'plm' | 'weno5'} */
+  double theta;        /* config_solver{theta} (PLM minmod) */
+  int    is_mode;      /* config_solver{IS = 'js96' | 'b08' | 'sz10'} */
+  double sz10A;        /* config_solver{sz10A} */
+  int    riemann;      /* set_riemann('hll' | 'hllc' | 'hlld') */
+  int    rk;           /* set_advance: 1 'single', 2 'rk2', 3 'rk3', 4 'rk4' */
+  double pfloor;       /* config_solver{pfloor}, disabled when <= 0 */
+  int    ereset;       /* config_solver{ereset} */
+  double preset;       /* config_solver{preset} */
+  double dreset;       /* config_solver{dreset} */
+  int    precision;    /* MGPU_PREC_FP64: plain path, reference arithmetic;
+                          MGPU_PREC_FP32: FP32 bulk, FP64 c2p polish / magnetic field / dt */
+  int    learned_c2p;  /* 1: first c2p attempt starts from the network set by
+                          mgpu_set_c2p_network (Newton polish, reference ladder as fallback) */
+} mgpu_config;
+
+typedef struct {
+  double max_lambda;          /* RiemannSolver::MaxLambda of the last advance */
+  double dt;                  /* dt of the last advance */
+  int    errors;              /* failed zones of the last advance (as Mara.advance returns) */
+  int    committed;           /* 1 if the last advance replaced the primitive state */
+  unsigned long long c2p_calls, c2p_iters;          /* zone c2p calls and Newton iterations */
+  unsigned long long c2p_attempt[6];                /* attempts used: [1..4] ladder rung,
+                                                       [5] learned guess rejected */
+  unsigned long long face_c2p_calls, face_c2p_iters; /* HLL-state c2p inside HLLD */
+  unsigned long long hlld_ok, hlld_hllc, pcm_retry;  /* HLLD successes / HLLC fallbacks /
+                                                        PCM retries of a face */
+} mgpu_stats;
+
+/* Defaults of a freshly started reference plus set_fluid('rmhd'), gamma 4/3, PLM theta 2,
+ * HLLD, RK2, FP64 (Mara/hydro.cpp:18-32,70-78; Mara/weno.c:10-12; Mara/rmhd-c2p.c:104). */
+int mgpu_default_config(mgpu_config *cfg);
+
+/* replaces luaC_Mara_start (Mara/mara.cpp:271-287) + the set_* selectors */
+int mgpu_create(const mgpu_config *cfg, mgpu_solver **out);
+/* replaces luaC_Mara_close (Mara/mara.cpp:288-295) */
+int mgpu_destroy(mgpu_solver *h);
+/* Use an existing CUDA stream (cudaStream_t passed as void*); NULL = the handle's own. */
+int mgpu_set_stream(mgpu_solver *h, void *stream);
+const char *mgpu_last_error(const mgpu_solver *h);
+
+/* replaces luaC_set_domain (Mara/mara.cpp:726-755): x0/x1/N have nd entries; nq must be 8;
+ * periodic boundaries (set_boundary('periodic')) with N_d >= ng on every axis. */
+int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const int *N, int nd, int nq,
+                    int ng);
+/* SimpleCartesianDomain::GetNumberOfZones (guard zones included, Mara/simple-cart.hpp:31) */
+int mgpu_num_zones(const mgpu_solver *h, long long *nzones);
+
+/* Primitive state (AoS with guard zones, nzones*8 doubles).  Host or device pointers. */
+int mgpu_upload_prim(mgpu_solver *h, const double *host_aos);
+int mgpu_download_prim(mgpu_solver *h, double *host_aos);
+int mgpu_upload_prim_device(mgpu_solver *h, const void *dev_aos);
+int mgpu_download_prim_device(mgpu_solver *h, void *dev_aos);
+
+/* replaces luaC_Mara_advance (Mara/mara.cpp:297-341) on the device-resident state:
+ * returns in *errors the number of failed zones (state unchanged when > 0).  Synchronous. */
+int mgpu_advance(mgpu_solver *h, double dt, int *errors);
+/* Mara.advance(buf, dt) exactly: copies the host buffer in, advances, copies it back when
+ * errors == 0; *kzps is 1e-3 * zones (guards included) / wall seconds of the call. */
+int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors);
+/* Enqueue n advances without host synchronisation: dt_mode 0 uses `dt` for every step,
+ * dt_mode 1 takes each step's dt = cfl*min_dx/MaxLambda of the step before (the first step
+ * uses the MaxLambda left by the previous advance).  A step that fails is not committed;
+ * later steps then restart from the last committed state.  Read the outcome with
+ * mgpu_get_stats after mgpu_synchronize. */
+int mgpu_advance_async(mgpu_solver *h, int n, int dt_mode, double dt, double cfl);
+int mgpu_synchronize(mgpu_solver *h);
+
+/* replaces luaC_Mara_get_timestep (Mara/mara.cpp:374-381) */
+int mgpu_get_timestep(mgpu_solver *h, double cfl, double *dt);
+int mgpu_get_stats(mgpu_solver *h, mgpu_stats *stats);
+
+/* Mara.set_primitive (Mara/mara.cpp:1284-1295): sets the array the measures read. */
+int mgpu_set_primitive(mgpu_solver *h, const double *host_aos);
+/* Mara.measure.mean_max_divB / max_lorentz_factor (Mara/mara.cpp:2232-2324) on the
+ * measured primitive array (the last RK stage's primitives after an advance, as in the
+ * reference, or the array given to mgpu_set_primitive). */
+int mgpu_measure_divB(mgpu_solver *h, double *mean, double *max);
+int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax);
+
+/* Kernel timing (no counterpart in the reference): while enabled, every kernel launch of an
+ * advance is bracketed by CUDA events on the handle's stream.  Classes: 0 begin/commit,
+ * 1 P->U, 2 c2p, 3 flux sweep, 4 CT+divergence+RK update.  mgpu_profile_read synchronizes
+ * and returns per class the summed milliseconds, the number of launches and the work units
+ * (faces for the flux class, interior zones otherwise); it then starts a new window. */
+int mgpu_profile_enable(mgpu_solver *h, int capacity);
+int mgpu_profile_disable(mgpu_solver *h);
+int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long *units);
+
+/* Learned c2p initial guess: weights of the packed network (layout in ctf_b200/csrc/
+ * c2p_mlp_net.cuh), copied to the device.  No counterpart in the reference. */
+int mgpu_set_c2p_network(mgpu_solver *h, const float *params, long long count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

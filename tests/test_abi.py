@@ -1,0 +1,60 @@
+"""The C-ABI library loads and exports every entry point include/mara_gpu.h declares
+(CPU-only: no compute call needs a GPU here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from ctf_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for hdr in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if hdr.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", hdr)).read()
+            names += re.findall(r"^\s*(?:int|const char \*|void)\s+(mgpu_\w+)\s*\(", text, re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "mgpu_advance" in names and "mgpu_create" in names and len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.build())
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    missing = [n for n in declared_functions() if n not in _lib.SIGNATURES]
+    assert not missing, missing
+
+
+def test_default_config_is_the_reference_defaults():
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    assert lib.mgpu_default_config(ctypes.byref(c)) == 0
+    assert c.gamma == 4.0 / 3.0 and c.theta == 2.0 and c.sz10A == 50.0 and c.pfloor == -1.0
+    assert c.recon == 1 and c.riemann == 2 and c.rk == 2 and c.precision == 0
+
+
+def test_bad_config_is_rejected_without_a_gpu():
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    c.rk = 7
+    h = ctypes.c_void_p()
+    assert lib.mgpu_create(ctypes.byref(c), ctypes.byref(h)) == 1   # MGPU_ERR_ARG
+    assert not h.value
+
+
+def test_null_handle_is_an_argument_error():
+    lib = _lib.load()
+    assert lib.mgpu_advance(None, 0.0, None) == 1
+    assert lib.mgpu_destroy(None) == 0

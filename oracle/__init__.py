@@ -23,6 +23,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_port", "liboracle_port.so")
+PORT_PERTURBED_SO = os.path.join(HERE, "_port", "liboracle_port_perturbed.so")
 REF_SO = os.path.join(HERE, "_ref", "libmara_ref.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -89,10 +90,11 @@ class _PortStats(ctypes.Structure):
 class PortOracle:
     """The C restatement (``oracle/port/mara_port.c``)."""
 
-    def __init__(self, scheme: Scheme):
-        if not os.path.exists(PORT_SO):
+    def __init__(self, scheme: Scheme, perturbed_libm: bool = False):
+        so = PORT_PERTURBED_SO if perturbed_libm else PORT_SO
+        if not os.path.exists(so):
             build("port")
-        self.lib = ctypes.CDLL(PORT_SO)
+        self.lib = ctypes.CDLL(so)
         self.scheme = scheme
         c = _PortConfig()
         self.lib.port_default_config(ctypes.byref(c))

@@ -21,6 +21,15 @@ enum { C2P_SUCCESS, C2P_CONS_NAN, C2P_CONS_NEG_DENSITY, C2P_CONS_NEG_ENERGY,
 
 #define SGN(x) (((x) > 0) - ((x) < 0))
 
+/* Conditioning probe (oracle variant built with -DPORT_PERTURB_LIBM only): moves each libm
+ * result of the wave-speed quartic by one ulp, to measure how sensitive the reference's own
+ * result is to the last bit of pow/acos/cos/sin. */
+#ifdef PORT_PERTURB_LIBM
+#define LIBM(x) nextafter((x), INFINITY)
+#else
+#define LIBM(x) (x)
+#endif
+
 void port_default_config(port_config *c)
 {
   memset(c, 0, sizeof(*c));
@@ -276,21 +285,21 @@ static void cubic(double c3, double c2, double c1, double c0, double *x1, double
   const double delta = q * q * q + r * r;
   if (delta > 0.0) {
     double s1 = r + sqrt(delta);
-    s1 = (s1 >= 0.0) ? pow(s1, 1. / 3.) : -pow(-s1, 1. / 3.);
+    s1 = (s1 >= 0.0) ? LIBM(pow(s1, 1. / 3.)) : -LIBM(pow(-s1, 1. / 3.));
     double s2 = r - sqrt(delta);
-    s2 = (s2 >= 0.0) ? pow(s2, 1. / 3.) : -pow(-s2, 1. / 3.);
+    s2 = (s2 >= 0.0) ? LIBM(pow(s2, 1. / 3.)) : -LIBM(pow(-s2, 1. / 3.));
     *x1 = (s1 + s2) - a2 / 3.0;
     *x2 = *x3 = -0.5 * (s1 + s2) - a2 / 3.0;
     *nr = 1;
   } else if (delta < 0.0) {
-    const double theta = acos(r / sqrt(-q * q * q)) / 3.0;
-    const double costh = cos(theta), sinth = sin(theta), sq = sqrt(-q);
+    const double theta = LIBM(acos(r / sqrt(-q * q * q))) / 3.0;
+    const double costh = LIBM(cos(theta)), sinth = LIBM(sin(theta)), sq = sqrt(-q);
     *x1 = 2.0 * sq * costh - a2 / 3.0;
     *x2 = -sq * costh - a2 / 3.0 - sqrt(3.) * sq * sinth;
     *x3 = -sq * costh - a2 / 3.0 + sqrt(3.) * sq * sinth;
     *nr = 3;
   } else {
-    const double s = (r >= 0.0) ? pow(r, 1. / 3.) : -pow(-r, 1. / 3.);
+    const double s = (r >= 0.0) ? LIBM(pow(r, 1. / 3.)) : -LIBM(pow(-r, 1. / 3.));
     *x1 = 2.0 * s - a2 / 3.0;
     *x2 = *x3 = -s - a2 / 3.0;
     *nr = 3;

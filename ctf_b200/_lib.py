@@ -71,6 +71,8 @@ SIGNATURES = {
     "mgpu_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_longlong)]),
     "mgpu_set_c2p_network": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_longlong]),
+    "mgpu_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), _dp, _dp, _ip, ctypes.c_int, _vp, _vp,
+                                            ctypes.c_double, _ip, _dp, _vp, ctypes.c_char_p, ctypes.c_int]),
 }
 
 

@@ -127,6 +127,24 @@ int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long
  * c2p_mlp_net.cuh), copied to the device.  No counterpart in the reference. */
 int mgpu_set_c2p_network(mgpu_solver *h, const float *params, long long count);
 
+/* Allocation-free advance (no counterpart in the reference).  For callers that may not
+ * allocate device memory -- allocation-free sections of a larger application, real-time
+ * loops, hosts that hand out only pre-owned buffers: one FP64 advance of a box of at most
+ * MGPU_NOALLOC_MAX_ZONES guarded zones, using working arrays kept in a fixed ~7.8 MiB region
+ * of the library's own device memory (present on every GPU that loads the library, for the
+ * life of the process) instead of cudaMalloc.  The caller passes device AoS primitives with
+ * guard zones in (dev_prim_in) and out (dev_prim_out, written only when *errors == 0) and a
+ * stream (NULL = the default stream); cfg must select MGPU_PREC_FP64 without learned_c2p;
+ * Ng is 3.  The call is synchronous and returns the reference's error count and MaxLambda.
+ * Larger boxes are rejected with MGPU_ERR_ARG and a message in errbuf.  The first call on
+ * each device looks up that device's address of the region (cudaGetSymbolAddress); make it
+ * before any stream capture.  All calls share the region: calls whose work overlaps on the
+ * GPU (several streams or host threads) race and must be serialised by the caller. */
+#define MGPU_NOALLOC_MAX_ZONES 11520
+int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, const double *x1, const int *N, int nd,
+                         const void *dev_prim_in, void *dev_prim_out, double dt, int *errors,
+                         double *max_lambda, void *stream, char *errbuf, int errbuf_len);
+
 #ifdef __cplusplus
 }
 #endif

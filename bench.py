@@ -213,6 +213,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -238,12 +239,23 @@ def main():
     n, ic_kind, scheme_kw = WORKLOADS[args.workload]
     P0 = make_ic(ic_kind, n, seed=rank)
     stream = torch.cuda.Stream()
-    results = {}
-    states = {}
-    precisions = ["fp32"] if args.skip_fp64 else ["fp32", "fp64"]
+    net = None
+    net_path = os.path.join(ROOT, "ctf_b200", "data", "c2p_net.npz")
+    if os.path.exists(net_path) and not args.no_learned:
+        from ctf_b200.train_c2p import load as load_net
+        net = load_net(net_path)
+    # (precision, learned): FP64 first -- its primed MaxLambda sets the dt all runs share
+    runs = [("fp64", False)] if not args.skip_fp64 else []
+    runs.append(("fp32", False))
+    if net is not None:
+        runs.append(("fp32", True))
+    results, states, solvers = {}, {}, {}
     dt_fixed = None
-    for prec in reversed(precisions):   # FP64 first: its primed MaxLambda sets the shared dt
-        s = Solver(Scheme(precision=prec, **scheme_kw), n, stream=stream.cuda_stream)
+    for prec, learned in runs:
+        key = prec + ("+learned" if learned else "")
+        s = Solver(Scheme(precision=prec, learned_c2p=learned, **scheme_kw), n, stream=stream.cuda_stream)
+        if learned:
+            s.set_c2p_network(net)
         s.upload(P0)
         assert s.advance(0.0) == 0, "priming advance failed"
         if dt_fixed is None:
@@ -261,33 +273,43 @@ def main():
             ms = float(t.item())
         st = s.stats()
         zones = int(np.prod(n))
-        results[prec] = {"ms_total": ms, "ms_per_step": ms / args.steps,
-                         "value": zones * args.steps * world / (ms * 1e-3), "prof": prof, "stats": st,
-                         "clocks": clk.summary()}
-        states[prec] = s.download()
+        results[key] = {"ms_total": ms, "ms_per_step": ms / args.steps,
+                        "value": zones * args.steps * world / (ms * 1e-3), "prof": prof, "stats": st,
+                        "clocks": clk.summary()}
+        states[key] = s.download()
         s.profile_disable()
-        if prec == "fp32":
-            solver_fp32 = s
-        else:
+        solvers[key] = s
+    head_key = "fp32+learned" if "fp32+learned" in results else "fp32"
+    solver_fp32 = solvers[head_key]
+    for k, s in solvers.items():
+        if k != head_key:
             s.close()
 
-    head = results["fp32"]
+    head = results[head_key]
     out = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL,
-                   "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt",
+                   "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
+                                + ("; learned c2p guess (bf16 tcgen05 MLP)" if head_key.endswith("learned") else ""),
                    "dt": dt_fixed, "l2": "every state array > 126 MB L2 (no flush needed)",
                    "parallelism": f"{world} independent replica(s)"},
         "gpu_launches": launches_per_step(len(n), scheme_kw["advance"]) * args.steps,
         "clocks": head["clocks"],
     }
+    def c2p_it(k):
+        st = results[k]["stats"]
+        return st["c2p_iters"] / max(st["c2p_calls"], 1)
+    out["runs"] = {k: {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                       "c2p_iters_per_call": c2p_it(k),
+                       "kernel_ms_per_step": {c: r["prof"][c]["ms"] / args.steps for c in r["prof"]}}
+                   for k, r in results.items()}
     if "fp64" in results:
         out["fp64_plain"] = {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
                              "clocks": results["fp64"]["clocks"]}
         out["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
-        out["l1_rel_vs_fp64"] = rel_l1(states["fp32"], states["fp64"], len(n))
+        out["l1_rel_vs_fp64"] = rel_l1(states[head_key], states["fp64"], len(n))
 
     # roofline of the dominant kernel (event-timed inside the timed region)
     peaks = {}
@@ -311,7 +333,7 @@ def main():
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
                        "algorithmic_bytes_per_unit": per_unit[dom]}
-    out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "face_c2p_calls",
+    out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "c2p_attempt", "face_c2p_calls",
                                                       "face_c2p_iters", "hlld_ok", "hlld_hllc", "pcm_retry")}
 
     # end to end through Mara.advance(buf, dt) semantics with pinned host buffers

@@ -66,11 +66,22 @@ SIGNATURES = {
     "mgpu_set_primitive": (ctypes.c_int, [_vp, _dp]),
     "mgpu_measure_divB": (ctypes.c_int, [_vp, _dp, _dp]),
     "mgpu_max_lorentz_factor": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_divB_state": (ctypes.c_int, [_vp, _dp, _dp]),
     "mgpu_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
     "mgpu_profile_disable": (ctypes.c_int, [_vp]),
     "mgpu_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_longlong)]),
     "mgpu_set_c2p_network": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_longlong]),
+    "mgpu_mlp_param_count": (ctypes.c_int, []),
+    "mgpu_c2p_harvest": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_mlp_work_floats": (ctypes.c_longlong, [ctypes.c_longlong]),
+    "mgpu_mlp_loss_grad": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, _vp, _vp, _dp]),
+    "mgpu_mlp_train": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_int, _vp, _dp]),
+    "mgpu_mlp_forward": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
+    "mgpu_mlp_forward_tc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _vp, ctypes.c_longlong, _vp]),
+    "mgpu_mlp_tc_image_bytes": (ctypes.c_int, []),
+    "mgpu_mlp_build_tc_image": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _vp]),
     "mgpu_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), _dp, _dp, _ip, ctypes.c_int, _vp, _vp,
                                             ctypes.c_double, _ip, _dp, _vp, ctypes.c_char_p, ctypes.c_int]),
 }

@@ -38,6 +38,7 @@ struct mgpu_solver {
   double *red_host = nullptr;   // pinned
   float *mlp = nullptr;         // learned c2p network (device)
   long long mlp_count = 0;
+  void *mlp_tc = nullptr;       // its tensor-core image (device)
   // kernel timing
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_tag;
@@ -81,7 +82,9 @@ PhysParams phys(const mgpu_solver *h)
   p.recon = h->cfg.recon;
   p.riemann = h->cfg.riemann;
   p.learned = h->cfg.learned_c2p && h->mlp != nullptr;
+  p.learned_faces = 0;
   p.mlp = h->mlp;
+  p.mlp_tc = h->mlp_tc;
   return p;
 }
 
@@ -123,7 +126,16 @@ int ensure_ready(mgpu_solver *h)
 
 // ---- measures (Mara/mara.cpp:2232-2324) on an 8 x T face array ------------------------------
 template <class T>
+__device__ __forceinline__ void k_divB_body(Grid g, const T *P, double *partial);
+
+template <class T>
 __global__ void k_divB(Grid g, const T *P, double *partial)
+{
+  k_divB_body<T>(g, P, partial);
+}
+
+template <class T>
+__device__ __forceinline__ void k_divB_body(Grid g, const T *P, double *partial)
 {
   // corner-centred divergence over i in [ng, G0-ng-1) etc. (interior corners but the last)
   const int ng = g.ng;
@@ -170,6 +182,13 @@ __global__ void k_divB(Grid g, const T *P, double *partial)
     partial[2 * blockIdx.x] = ss[0];
     partial[2 * blockIdx.x + 1] = sm[0];
   }
+}
+
+// Corner divergence of a state's FP64 magnetic field (components 5..7 at B + (q-5)*cs).
+__global__ void k_divB_state(Grid g, const double *B, double *partial)
+{
+  // k_divB reads P[q*cs + z] for q = 5..7: shift the base so that q = 5 lands on B[0].
+  k_divB_body<double>(g, B - 5 * g.cs, partial);
 }
 
 template <class T>
@@ -282,6 +301,7 @@ int mgpu_destroy(mgpu_solver *h)
   free_buffers(h);
   prof_free(h);
   if (h->mlp) cudaFree(h->mlp);
+  if (h->mlp_tc) cudaFree(h->mlp_tc);
   if (h->ctl) cudaFree(h->ctl);
   if (h->ctl_host) cudaFreeHost(h->ctl_host);
   if (h->red_host) cudaFreeHost(h->red_host);
@@ -500,6 +520,7 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
   if (rc) return rc;
   rc = read_ctl(h);
   if (rc) return rc;
+  if (h->ctl_host->tc_fault) return fail(h, MGPU_ERR_CUDA, "a tensor-core wait of the learned c2p timed out");
   if (errors) *errors = errors_of(*h->ctl_host, h->cfg.rk);
   return MGPU_OK;
 }
@@ -604,6 +625,34 @@ int mgpu_measure_divB(mgpu_solver *h, double *mean, double *max)
   return MGPU_OK;
 }
 
+int mgpu_measure_divB_state(mgpu_solver *h, double *mean, double *max)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (h->g.nd < 2) {
+    *mean = 0.0;
+    *max = 0.0;
+    return MGPU_OK;
+  }
+  CK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const double *B = h->b.Pc_B[h->ctl_host->cur];
+  k_divB_state<<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, B, h->red);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->red_host, h->red, sizeof(double) * 2 * RED_BLOCKS, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  double sum = 0.0, mx = 0.0;
+  for (int b = 0; b < RED_BLOCKS; ++b) {
+    sum += h->red_host[2 * b];
+    mx = fmax(mx, h->red_host[2 * b + 1]);
+  }
+  long long glb = 1;
+  for (int d = 0; d < h->g.nd; ++d) glb *= h->N[d];
+  *mean = (sum / (double) h->g.nz) / (double) glb;
+  *max = mx;
+  return MGPU_OK;
+}
+
 int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax)
 {
   int rc = ensure_ready(h);
@@ -664,16 +713,36 @@ int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long
   return MGPU_OK;
 }
 
+// Grid, buffers and stream of a solver, for the learned-c2p harvest (c2p_mlp.cu).
+int mgpu_internal_state(mgpu_solver *h, Grid *g, AdvanceBuffers *b, Ctl **ctl, void **stream, int *is32,
+                        double *gamma)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  *g = h->g;
+  *b = h->b;
+  *ctl = h->ctl;
+  *stream = (void *) h->stream;
+  *is32 = fp32(h);
+  *gamma = h->cfg.gamma;
+  return MGPU_OK;
+}
+
 int mgpu_set_c2p_network(mgpu_solver *h, const float *params, long long count)
 {
-  if (!h || !params || count <= 0) return MGPU_ERR_ARG;
-  if (h->mlp) {
-    cudaStreamSynchronize(h->stream);
-    cudaFree(h->mlp);
-    h->mlp = nullptr;
-  }
+  if (!h || !params) return MGPU_ERR_ARG;
+  if (count != mgpu_mlp_param_count()) return fail(h, MGPU_ERR_ARG, "network has the wrong number of parameters");
+  cudaStreamSynchronize(h->stream);
+  if (h->mlp) cudaFree(h->mlp);
+  if (h->mlp_tc) cudaFree(h->mlp_tc);
+  h->mlp = nullptr;
+  h->mlp_tc = nullptr;
   CK(cudaMalloc((void **) &h->mlp, count * sizeof(float)));
   CK(cudaMemcpy(h->mlp, params, count * sizeof(float), cudaMemcpyHostToDevice));
+  std::vector<unsigned char> img(mgpu_mlp_tc_image_bytes());
+  mgpu_mlp_build_tc_image(params, img.data());
+  CK(cudaMalloc(&h->mlp_tc, img.size()));
+  CK(cudaMemcpy(h->mlp_tc, img.data(), img.size(), cudaMemcpyHostToDevice));
   h->mlp_count = count;
   return MGPU_OK;
 }

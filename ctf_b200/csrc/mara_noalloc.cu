@@ -180,7 +180,9 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   A.pp.recon = cfg->recon;
   A.pp.riemann = cfg->riemann;
   A.pp.learned = 0;
+  A.pp.learned_faces = 0;
   A.pp.mlp = nullptr;
+  A.pp.mlp_tc = nullptr;
   A.rk = cfg->rk;
   A.ereset = cfg->ereset;
   A.preset = cfg->preset;

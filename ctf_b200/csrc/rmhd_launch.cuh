@@ -4,6 +4,7 @@
 // Nothing is read back: the host learns the outcome from the control block when it asks.
 #pragma once
 #include "rmhd_step.cuh"
+#include "rmhd_step_tc.cuh"
 
 namespace mgpu {
 
@@ -41,9 +42,20 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
   T *PA = (T *) b.PA;
   const T *F = (const T *) b.F[0], *G = (const T *) b.F[1], *H = (const T *) b.F[2];
 
-  const unsigned zb = 256, cb = 128, fb = 128;
+  const unsigned zb = 256, fb = 128;
+  // learned guess on the tensor cores: persistent c2p kernel, at most 3 CTAs per SM
+  const bool tc_c2p = A.pp.learned && A.pp.mlp_tc;
+  const long long ntiles = (g.ninterior + 127) / 128;
+  const unsigned tcgrid = (unsigned) (ntiles < 148 * 3 ? ntiles : 148 * 3);
+  auto c2p = [&](StateCPtr<T> Uin, int s, int zero_guess, int final) {
+    if (tc_c2p)
+      k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
+                                                                final, A.ereset, A.preset, A.dreset);
+    else
+      k_cons_to_prim<T><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
+          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
+  };
   const unsigned zgrid = (unsigned) ((g.ninterior + zb - 1) / zb);
-  const unsigned cgrid = (unsigned) ((g.ninterior + cb - 1) / cb);
 
   LaunchProfiler *pr = A.prof;
   {
@@ -60,8 +72,7 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
     const StatePtr<T> Uin = s == 0 ? U0 : U1;
     {
       ProfScope ps(pr, st, KC_C2P, g.ninterior);
-      k_cons_to_prim<T><<<cgrid, cb, 0, st>>>(g, StateCPtr<T>{Uin.bulk, Uin.B}, PA, Pc0, Pc1, A.pp, A.ctl, s, s == 0,
-                                              0, A.ereset, A.preset, A.dreset);
+      c2p(StateCPtr<T>{Uin.bulk, Uin.B}, s, s == 0, 0);
     }
     for (int d = 1; d <= g.nd; ++d) {
       const long long S = g.s[d - 1];
@@ -69,7 +80,9 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
       if (nf <= 0) continue;
       const unsigned fgrid = (unsigned) ((nf + fb - 1) / fb);
       ProfScope ps(pr, st, KC_FLUX, nf);
-      k_flux<T><<<fgrid, fb, 0, st>>>(g, d, PA, (T *) b.F[d - 1], A.pp, A.ctl, s);
+      if (d == 1) k_flux<T, 1><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[0], A.pp, A.ctl, s);
+      else if (d == 2) k_flux<T, 2><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[1], A.pp, A.ctl, s);
+      else k_flux<T, 3><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[2], A.pp, A.ctl, s);
     }
     const StageKind kind = stage_kind(A.rk, s);
     UpdateArgs ua{kind.combine, kind.c};
@@ -89,8 +102,7 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
   }
   {
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
-    k_cons_to_prim<T><<<cgrid, cb, 0, st>>>(g, StateCPtr<T>{U0.bulk, U0.B}, PA, Pc0, Pc1, A.pp, A.ctl, ns, 0, 1,
-                                            A.ereset, A.preset, A.dreset);
+    c2p(StateCPtr<T>{U0.bulk, U0.B}, ns, 0, 1);
   }
   {
     ProfScope ps(pr, st, KC_BEGIN, 1);

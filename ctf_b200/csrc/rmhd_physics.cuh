@@ -337,7 +337,7 @@ __device__ __forceinline__ int c2p_reconstruct(const C2PState &s, double Z, doub
 }
 
 // Anton et al. (2006) eqs 84-85, 2-D Newton in (Z, W) (Mara/rmhd-c2p.c:232-303).
-static __device__ __noinline__ int c2p_anton2dzw(const C2PState &s, double Z, double W, double *P, int &iters)
+__device__ __forceinline__ int c2p_anton2dzw(const C2PState &s, double Z, double W, double *P, int &iters)
 {
   const double D = s.D, B2 = s.B2, BS2 = s.BS2, S2 = s.S2, gamf = s.gamf, Tau = s.Tau;
   double error = 1.0;
@@ -368,8 +368,48 @@ static __device__ __noinline__ int c2p_anton2dzw(const C2PState &s, double Z, do
   return c2p_reconstruct(s, Z, W, P);
 }
 
+// The same Anton et al. Newton iteration with the divisions replaced by three reciprocals
+// per iteration (1/W, 1/Z, 1/det); algebraically identical, rounded differently.  Used by
+// the FP32-bulk path, whose c2p is an FP64 polish judged against the FP64 path rather than
+// the reference's bit pattern.
+__device__ __forceinline__ int c2p_anton2dzw_fast(const C2PState &s, double Z, double W, double *P, int &iters)
+{
+  const double D = s.D, B2 = s.B2, BS2 = s.BS2, S2 = s.S2, gamf = s.gamf, Tau = s.Tau;
+  const double iD = 1.0 / D;
+  double iW = 1.0 / W, iZ = 1.0 / Z;
+  double error = 1.0;
+  iters = 0;
+  while (error > 1e-12) {
+    const double W2 = W * W, Z2 = Z * Z, Z3 = Z * Z2;
+    const double iW2 = iW * iW, iW3 = iW2 * iW, iZ2 = iZ * iZ, iZ3 = iZ2 * iZ;
+    const double Pre = D * iW * (Z * iD * iW - 1.0) * gamf;
+    const double BZ = B2 + Z;
+    const double df0dZ = 2 * BZ * (BS2 * W2 + (W2 - 1) * Z3) * iW2 * iZ3;
+    const double df0dW = 2 * BZ * BZ * iW3;
+    const double df1dZ = 1.0 + BS2 * iZ3 - gamf * iW2;
+    const double df1dW = (B2 + (2 * Z - D * W) * gamf) * iW3;
+    const double f0 = -S2 + BZ * BZ * (W2 - 1) * iW2 - (2 * Z + B2) * BS2 * iZ2;
+    const double f1 = -Tau + Z + B2 - Pre - 0.5 * B2 * iW2 - 0.5 * BS2 * iZ2 - D;
+    const double idet = 1.0 / (df0dZ * df1dW - df0dW * df1dZ);
+    const double dZ = -(df1dW * f0 - df0dW * f1) * idet;
+    const double dW = -(df0dZ * f1 - df1dZ * f0) * idet;
+    double Zn = Z + dZ, Wn = W + dW;
+    Zn = (Zn > 0.0) ? Zn : -Zn;
+    Zn = (Zn < 1e20) ? Zn : Z;
+    Wn = (Wn > 1.0) ? Wn : 1.0;
+    Wn = (Wn < 1e12) ? Wn : 1e12;
+    Z = Zn;
+    W = Wn;
+    iZ = 1.0 / Z;
+    iW = 1.0 / W;
+    error = fabs(dZ * iZ) + fabs(dW * iW);
+    if (++iters == 250) return C2P_MAXITER;
+  }
+  return c2p_reconstruct(s, Z, W, P);
+}
+
 // Noble et al. (2006) 1-D Newton in Z (Mara/rmhd-c2p.c:311-376).
-static __device__ __noinline__ int c2p_noble1dw(const C2PState &s, double Z, double *P, int &iters)
+__device__ __forceinline__ int c2p_noble1dw(const C2PState &s, double Z, double *P, int &iters)
 {
   const double D = s.D, B2 = s.B2, BS2 = s.BS2, S2 = s.S2, gamf = s.gamf, Tau = s.Tau;
   double error = 1.0;
@@ -416,14 +456,50 @@ struct C2PTally {
 };
 
 // Optional learned initial guess: (Z, W) from the packed network; defined in c2p_mlp.cuh.
-__device__ bool c2p_learned_guess(const void *mlp, const C2PState &s, double &Z, double &W);
+__device__ __forceinline__ bool c2p_learned_guess(const void *net, const C2PState &s, double &Z, double &W);
+
+// The ladder's rungs 2-4 (previous prim -> Anton; estimate -> Noble; previous prim ->
+// Noble), reached only when the first attempt fails: kept out of line, state by value.
+struct C2PRungs {
+  double P[8];
+  int err, iters, attempt;
+};
+static __device__ __noinline__ C2PRungs c2p_rungs(const C2PState s, C2PRungs r)
+{
+  double Z, W;
+  int it = 0;
+  r.err = 1;
+  r.iters = 0;
+  c2p_from_prim(s, r.P, Z, W);
+  r.err = c2p_anton2dzw(s, Z, W, r.P, it);
+  r.iters += it;
+  r.attempt = 2;
+  if (r.err) {
+    c2p_estimate(s, Z, W);
+    r.err = c2p_noble1dw(s, Z, r.P, it);
+    r.iters += it;
+    r.attempt = 3;
+  }
+  if (r.err) {
+    c2p_from_prim(s, r.P, Z, W);
+    r.err = c2p_noble1dw(s, Z, r.P, it);
+    r.iters += it;
+    r.attempt = 4;
+  }
+  return r;
+}
 
 // AdiabaticIdealRmhd::ConsToPrim gamma-law ladder (Mara/rmhd.cpp:103-176).  P holds the
 // previous primitive state on entry (second guess) and is written only on success.  With a
-// learned network the first attempt starts from its guess instead (and the reference ladder
-// follows unchanged if that attempt fails).
+// learned network the first attempt starts from its guess instead, and the reference ladder
+// follows unchanged if that attempt fails.  The first Anton attempt is inlined (one call
+// site serves both the learned and the estimated starting point); the other rungs are not.
+// Guess (compile time): 0 = the per-thread network when pp.learned; 1 = the given (Zg, Wg)
+// when `have`; 2 = none (no network code is compiled in).
+template <bool Fast = false, int Guess = 0>
 __device__ __forceinline__ int cons_to_prim(const PhysParams &pp, const double *U, double *P,
-                                            C2PTally *tally = nullptr)
+                                            C2PTally *tally = nullptr, double Zg = 0.0, double Wg = 0.0,
+                                            bool have = true)
 {
   int error = check_cons(U);
   if (error) {
@@ -435,36 +511,40 @@ __device__ __forceinline__ int cons_to_prim(const PhysParams &pp, const double *
   s.gamf = (pp.gamma - 1.0) / pp.gamma;
   s.pfloor = pp.pfloor;
   c2p_new_state(s, U);
-  double Z, W;
-  int it = 0, total = 0, attempts = 1;
+  int total = 0, attempts = 1;
   error = 1;
-  if (pp.learned && pp.mlp && c2p_learned_guess(pp.mlp, s, Z, W)) {
-    error = c2p_anton2dzw(s, Z, W, P, it);
+  const bool use_net = (Guess == 1 && have) || (Guess == 0 && pp.learned && pp.mlp);
+  for (int a = use_net ? 0 : 1; a < 2 && error; ++a) {
+    double Z, W;
+    if (a == 0) {
+      if (Guess == 1) {
+        Z = Zg;
+        W = Wg;
+      } else if (Guess == 0) {
+        if (!c2p_learned_guess(pp.mlp, s, Z, W)) continue;
+      } else {
+        continue;
+      }
+    } else {
+      c2p_estimate(s, Z, W);
+    }
+    int it = 0;
+    error = Fast ? c2p_anton2dzw_fast(s, Z, W, P, it) : c2p_anton2dzw(s, Z, W, P, it);
     total += it;
-    if (error) attempts = 5;
+    if (error && a == 0) attempts = 5;
   }
   if (error) {
-    c2p_estimate(s, Z, W);
-    error = c2p_anton2dzw(s, Z, W, P, it);
-    total += it;
-  }
-  if (error) {
-    c2p_from_prim(s, P, Z, W);
-    error = c2p_anton2dzw(s, Z, W, P, it);
-    total += it;
-    attempts = attempts == 5 ? 5 : 2;
-  }
-  if (error) {
-    c2p_estimate(s, Z, W);
-    error = c2p_noble1dw(s, Z, P, it);
-    total += it;
-    attempts = attempts == 5 ? 5 : 3;
-  }
-  if (error) {
-    c2p_from_prim(s, P, Z, W);
-    error = c2p_noble1dw(s, Z, P, it);
-    total += it;
-    attempts = attempts == 5 ? 5 : 4;
+    C2PRungs r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.P[i] = P[i];
+    r = c2p_rungs(s, r);
+    total += r.iters;
+    error = r.err;
+    if (attempts != 5) attempts = r.attempt;
+    if (!error) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) P[i] = r.P[i];
+    }
   }
   if (tally) { tally->iters = total; tally->attempts = attempts; }
   return error;
@@ -557,14 +637,13 @@ template <class T> struct RiemannCount {
   int hlld_ok, hlld_fallback;
 };
 
-template <class T>
-__device__ __forceinline__ void dim_map(int dim, int &B1, int &B2, int &B3, int &S1, int &S2, int &S3,
-                                        int &v1, int &v2, int &v3)
-{
-  if (dim == 1) { B1 = Bx; B2 = By; B3 = Bz; S1 = Sx; S2 = Sy; S3 = Sz; v1 = vx; v2 = vy; v3 = vz; }
-  else if (dim == 2) { B1 = By; B2 = Bz; B3 = Bx; S1 = Sy; S2 = Sz; S3 = Sx; v1 = vy; v2 = vz; v3 = vx; }
-  else { B1 = Bz; B2 = Bx; B3 = By; S1 = Sz; S2 = Sx; S3 = Sy; v1 = vz; v2 = vx; v3 = vy; }
-}
+// Index permutation of a sweep direction (compile time, so that the permuted state arrays
+// stay in registers): (B1, B2, B3), (S1, S2, S3), (v1, v2, v3) as in the reference's
+// IntercellFlux switch (e.g. Mara/riemann_hlld-rmhd.cpp:199-217).
+template <int DIM> struct DimMap;
+template <> struct DimMap<1> { enum { B1 = Bx, B2 = By, B3 = Bz, S1 = Sx, S2 = Sy, S3 = Sz, v1 = vx, v2 = vy, v3 = vz }; };
+template <> struct DimMap<2> { enum { B1 = By, B2 = Bz, B3 = Bx, S1 = Sy, S2 = Sz, S3 = Sx, v1 = vy, v2 = vz, v3 = vx }; };
+template <> struct DimMap<3> { enum { B1 = Bz, B2 = Bx, B3 = By, S1 = Sz, S2 = Sx, S3 = Sy, v1 = vz, v2 = vx, v3 = vy }; };
 
 template <class T>
 __device__ __forceinline__ T face_lambda(T ap, T am)
@@ -573,8 +652,8 @@ __device__ __forceinline__ T face_lambda(T ap, T am)
 }
 
 // HllRiemannSolver::IntercellFlux at s = 0 (Mara/riemann_hll.cpp:19-64)
-template <class T>
-__device__ __noinline__ int riemann_hll(T gamma, const T *Pl, const T *Pr, T *F, int dim, T &ml)
+template <class T, int dim>
+__device__ __forceinline__ int riemann_hll(T gamma, const T *Pl, const T *Pr, T *F, T &ml)
 {
   T Ul[8], Ur[8], Fl[8], Fr[8], epl, eml, epr, emr;
   if (prim_to_cons(gamma, Pl, Ul)) return 1;
@@ -596,13 +675,28 @@ __device__ __noinline__ int riemann_hll(T gamma, const T *Pl, const T *Pr, T *F,
   return 0;
 }
 
-// HllcRmhdRiemannSolver::IntercellFlux at s = 0 (Mara/riemann_hllc-rmhd.cpp:26-178)
+// Contact speed of HLLC: the root (-b - sqrt(b^2 - 4ac)) / (2a) of a x^2 + b x + c, or -c/b
+// when |a| is below SMALL_A (Mara/riemann_hllc-rmhd.cpp:96,134).  In FP64 the reference's
+// expression is kept as written.  In FP32 it cancels catastrophically when a is small and
+// b < 0 (an error of ~eps * |b| / a), so the FP32 path uses the algebraically identical
+// 2c / (-b + sqrt(b^2 - 4ac)) there.
 template <class T>
-__device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F, int dim, T &ml)
+__device__ __forceinline__ T hllc_contact_speed(T a, T b, T c)
 {
   using Tol = RmhdTol<T>;
-  int B1, B2, B3, S1, S2, S3, v1, v2, v3;
-  dim_map<T>(dim, B1, B2, B3, S1, S2, S3, v1, v2, v3);
+  if (m_abs(a) < T(Tol::hllc_a)) return -c / b;
+  if (sizeof(T) == sizeof(double)) return (-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a);
+  const T sq = m_sqrt(b * b - T(4) * a * c);
+  return b <= T(0) ? T(2) * c / (-b + sq) : -(b + sq) / (T(2) * a);
+}
+
+// HllcRmhdRiemannSolver::IntercellFlux at s = 0 (Mara/riemann_hllc-rmhd.cpp:26-178)
+template <class T, int dim>
+__device__ __forceinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F, T &ml)
+{
+  using Tol = RmhdTol<T>;
+  using M = DimMap<dim>;
+  constexpr int B1 = M::B1, B2 = M::B2, B3 = M::B3, S1 = M::S1, S2 = M::S2, S3 = M::S3, v1 = M::v1;
   T Pl[8], Pr[8], Ul[8], Ur[8], Fl[8], Fr[8], epl, eml, epr, emr;
 #pragma unroll
   for (int i = 0; i < 8; ++i) { Pl[i] = pl[i]; Pr[i] = pr[i]; }
@@ -623,13 +717,13 @@ __device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F
     Uh[i] = (ap * Ur[i] - am * Ul[i] + (Fl[i] - Fr[i])) / (ap - am);
     Fh[i] = (ap * Fl[i] - am * Fr[i] + ap * am * (Ur[i] - Ul[i])) / (ap - am);
   }
-  T Ul_[8], Ur_[8], lc;
+  T Ul_[8], Ur_[8], lc, hllc_star_p;
   if (m_abs(Uh[B1]) > T(Tol::hllc_bx)) {
     const T BdFB = Uh[B2] * Fh[B2] + Uh[B3] * Fh[B3];
     const T a = Fh[tau] - BdFB;
     const T b = -Fh[S1] - Uh[tau] + (Uh[B2] * Uh[B2] + Uh[B3] * Uh[B3]) + (Fh[B2] * Fh[B2] + Fh[B3] * Fh[B3]);
     const T c = Uh[S1] - BdFB;
-    const T w1 = lc = (m_abs(a) < T(Tol::hllc_a)) ? -c / b : (-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a);
+    const T w1 = lc = hllc_contact_speed(a, b, c);
     const T w2 = (Uh[B2] * w1 - Fh[B2]) / Uh[B1];
     const T w3 = (Uh[B3] * w1 - Fh[B3]) / Uh[B1];
     const T b1 = Uh[B1], b2 = Uh[B2], b3 = Uh[B3];
@@ -637,6 +731,7 @@ __device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F
     const T vdv = w1 * w1 + w2 * w2 + w3 * w3;
     const T gm2 = T(1) / (T(1) - vdv);
     const T ps = Fh[S1] + b1 * b1 / gm2 - (Fh[tau] - b1 * vdB) * w1;
+    hllc_star_p = ps;
     Ul_[ddd] = (am - Pl[v1]) / (am - w1) * Ul[ddd];
     Ur_[ddd] = (ap - Pr[v1]) / (ap - w1) * Ur[ddd];
     Ul_[tau] = (am * Ul[tau] - Ul[S1] + ps * w1 - vdB * b1) / (am - w1);
@@ -654,8 +749,9 @@ __device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F
     const T a = Fh[tau];
     const T b = -Fh[S1] - Uh[tau];
     const T c = Uh[S1];
-    const T v1_ = lc = (m_abs(a) < T(Tol::hllc_a)) ? -c / b : (-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a);
+    const T v1_ = lc = hllc_contact_speed(a, b, c);
     const T p_ = -Fh[tau] * v1_ + Fh[S1];
+    hllc_star_p = p_;
     Ul_[ddd] = (am - Pl[v1]) / (am - v1_) * Ul[ddd];
     Ur_[ddd] = (ap - Pr[v1]) / (ap - v1_) * Ur[ddd];
     Ul_[tau] = (am * Ul[tau] - Ul[S1] + p_ * v1_) / (am - v1_);
@@ -674,6 +770,18 @@ __device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F
     Ur_[B3] = (ap - Pr[v1]) / (ap - v1_) * Ur[B3];
   }
   const T s = T(0);
+  // FP32 path only: a star state that rounding made unphysical (non-finite or superluminal
+  // contact, negative star pressure or density) takes the HLL flux at this face instead.
+  if (sizeof(T) < sizeof(double)) {
+    const bool bad = !(isfinite(lc) && m_abs(lc) < T(1) && hllc_star_p >= T(0) && Ul_[ddd] > T(0) &&
+                       Ur_[ddd] > T(0) && isfinite(Ul_[tau]) && isfinite(Ur_[tau]));
+    if (bad) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) F[i] = (s <= am) ? Fl[i] : (s <= ap ? Fh[i] : Fr[i]);
+      F[tau] -= F[ddd];
+      return 0;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     if (s <= am) F[i] = Fl[i];
@@ -683,6 +791,19 @@ __device__ __noinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F
   }
   F[tau] -= F[ddd];
   return 0;
+}
+
+// Out-of-line HLLC for the HLLD fallback (rare): arguments and result by value so that the
+// caller's face states stay in registers on its hot path.
+template <class T> struct Face8 { T v[8]; };
+template <class T> struct HllcOut { T F[8]; T ml; int err; };
+template <class T, int dim>
+static __device__ __noinline__ HllcOut<T> riemann_hllc_fallback(T gamma, Face8<T> pl, Face8<T> pr, T ml)
+{
+  HllcOut<T> o;
+  o.ml = ml;
+  o.err = riemann_hllc<T, dim>(gamma, pl.v, pr.v, o.F, o.ml);
+  return o;
 }
 
 // ---- HLLD (Mignone, Ugliano & Bodo 2009; Mara/riemann_hlld-rmhd.cpp) -------------------------
@@ -743,7 +864,7 @@ __device__ __forceinline__ void hlld_fill(const HlldEqn<T> &q, T p, T *Kl, T *Kr
 
 // HlldEquation48::Function (riemann_hlld-rmhd.cpp:422-452); returns non-zero on "throw".
 template <class T>
-__device__ __noinline__ int hlld_function(const HlldEqn<T> &q, T p, T &y)
+__device__ __forceinline__ int hlld_function(const HlldEqn<T> &q, T p, T &y)
 {
   using Tol = RmhdTol<T>;
   if (m_abs(q.PlBx - q.PrBx) > T(Tol::bjump)) return 1;
@@ -768,16 +889,22 @@ __device__ __forceinline__ int hlld_newton(const HlldEqn<T> &q, T &x)
 {
   using Tol = RmhdTol<T>;
   const int MaxIterations = 15;
+  const T dp = T(Tol::jac_dp);
   int worse = 0, it = 0;
   T eps = T(0), eps_last;
   do {
     eps_last = eps;
-    T y, f0, f1;
-    if (hlld_function(q, x, y)) return 1;
-    const T dp = T(Tol::jac_dp);
-    const T p0 = x - T(0.5) * dp, p1 = x + T(0.5) * dp;
-    if (hlld_function(q, p0, f0)) return 1;
-    if (hlld_function(q, p1, f1)) return 1;
+    // f(x), f(x - dp/2), f(x + dp/2): one evaluation site, three points
+    T y = T(0), f0 = T(0), f1 = T(0);
+#pragma unroll 1
+    for (int e = 0; e < 3; ++e) {
+      const T pe = e == 0 ? x : (e == 1 ? x - T(0.5) * dp : x + T(0.5) * dp);
+      T r;
+      if (hlld_function(q, pe, r)) return 1;
+      if (e == 0) y = r;
+      else if (e == 1) f0 = r;
+      else f1 = r;
+    }
     const T J = (f1 - f0) / dp;
     const T G = T(1) / J;
     T dx = T(0);
@@ -792,9 +919,53 @@ __device__ __forceinline__ int hlld_newton(const HlldEqn<T> &q, T &x)
   return 0;
 }
 
+// Secant iteration on equation 48 (the structure of SecantMethodSolver::Solve,
+// Mara/secant.cpp:19-60, which the reference constructs for this equation but does not
+// call): one evaluation per iteration instead of Newton's three.  Used by the FP32-bulk
+// path only; the FP64 path keeps the reference's Newton-Raphson.
+template <class T>
+__device__ __forceinline__ int hlld_secant(const HlldEqn<T> &q, T &x)
+{
+  using Tol = RmhdTol<T>;
+  const int MaxIterations = 15;
+  T x0 = x, x1 = x + T(Tol::jac_dp), y0 = T(0), y1 = T(0);
+  int worse = 0;
+#pragma unroll 1
+  for (int it = -2; it <= MaxIterations; ++it) {
+    // it == -2, -1: the two starting points; then one secant step per iteration
+    T xe;
+    if (it == -2) xe = x0;
+    else if (it == -1) xe = x1;
+    else xe = x1 - y1 * (x1 - x0) / (y1 - y0);
+    T r;
+    if (hlld_function(q, xe, r)) return 1;
+    if (isnan(r)) return 1;
+    if (it == -2) {
+      y0 = r;
+      if (m_abs(y0) < T(Tol::newton_eps)) return 0;
+      continue;
+    }
+    if (it >= 0) {
+      x0 = x1;
+      y0 = y1;
+      x1 = xe;
+    }
+    y1 = r;
+    if (it >= 0) {
+      worse += (m_abs(y1) > m_abs(y0));
+      if (worse >= 10) return 1;
+    }
+    if (m_abs(y1) <= T(Tol::newton_eps)) {
+      x = x1;
+      return 0;
+    }
+  }
+  return 1;
+}
+
 // ReconstructSolution (riemann_hlld-rmhd.cpp:453-575) at s = 0, flux only.
 template <class T>
-__device__ __noinline__ int hlld_reconstruct(const HlldEqn<T> &q, T p, T *F)
+__device__ __forceinline__ int hlld_reconstruct(const HlldEqn<T> &q, T p, T *F)
 {
   using Tol = RmhdTol<T>;
   T Kl[3], Kr[3], Bc[3], etaL, etaR, wL, wR;
@@ -901,7 +1072,7 @@ __device__ __forceinline__ int cons_to_prim_T(const PhysParams &pp, const T *U, 
   double Ud[8], Pd[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) { Ud[i] = double(U[i]); Pd[i] = double(P[i]); }
-  const int e = cons_to_prim(pp, Ud, Pd, tally);
+  const int e = cons_to_prim<(sizeof(T) < sizeof(double)), 2>(pp, Ud, Pd, tally);
   if (e == 0) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) P[i] = T(Pd[i]);
@@ -912,14 +1083,15 @@ __device__ __forceinline__ int cons_to_prim_T(const PhysParams &pp, const T *U, 
 // HlldRmhdRiemannSolver::IntercellFlux at s = 0 (riemann_hlld-rmhd.cpp:179-313).
 // Returns 1 when a face state is unphysical (the caller retries with PCM states);
 // `used_hllc` reports the fallback.
-template <class T>
-__device__ __noinline__ int riemann_hlld(const PhysParams &pp, const T *pl, const T *pr, T *f, int dim, T &ml,
+template <class T, int dim>
+__device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, const T *pr, T *f, T &ml,
                                          int &used_hllc, C2PTally *tally)
 {
   using Tol = RmhdTol<T>;
   const T gamma = T(pp.gamma);
-  int B1, B2, B3, S1, S2, S3, v1, v2, v3;
-  dim_map<T>(dim, B1, B2, B3, S1, S2, S3, v1, v2, v3);
+  using M = DimMap<dim>;
+  constexpr int B1 = M::B1, B2 = M::B2, B3 = M::B3, S1 = M::S1, S2 = M::S2, S3 = M::S3;
+  constexpr int v1 = M::v1, v2 = M::v2, v3 = M::v3;
   HlldEqn<T> q;
   T Pl[8], Pr[8], epl, eml, epr, emr;
   Pl[pre] = pl[pre]; Pr[pre] = pr[pre];
@@ -998,7 +1170,7 @@ __device__ __noinline__ int riemann_hlld(const PhysParams &pp, const T *pl, cons
     if (m_abs(Pl[Bx]) < T(Tol::bx_small) || m_abs(Pr[Bx]) < T(Tol::bx_small)) {
       rc = hlld_reconstruct(q, p_star, F);
     } else {
-      rc = hlld_newton(q, p_star);
+      rc = sizeof(T) < sizeof(double) ? hlld_secant(q, p_star) : hlld_newton(q, p_star);
       if (rc == 0) rc = hlld_reconstruct(q, p_star, F);
     }
     success = (rc == 0);
@@ -1016,7 +1188,14 @@ __device__ __noinline__ int riemann_hlld(const PhysParams &pp, const T *pl, cons
     return 0;
   }
   used_hllc = 1;
-  return riemann_hllc(gamma, pl, pr, f, dim, ml);
+  Face8<T> a, b;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) { a.v[i] = pl[i]; b.v[i] = pr[i]; }
+  const HllcOut<T> o = riemann_hllc_fallback<T, dim>(gamma, a, b, ml);
+  ml = o.ml;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) f[i] = o.F[i];
+  return o.err;
 }
 
 }  // namespace mgpu

@@ -14,6 +14,12 @@
 #include <stdint.h>
 #include "rmhd_physics.cuh"
 
+// Minimum resident blocks of 128 threads per SM requested for the flux sweep (caps its
+// registers at 65536 / (128 * MGPU_FLUX_MINB)).
+#ifndef MGPU_FLUX_MINB
+#define MGPU_FLUX_MINB 2
+#endif
+
 namespace mgpu {
 
 __device__ __forceinline__ bool stage_failed(const Ctl *ctl, int upto)
@@ -92,15 +98,11 @@ static __global__ void k_commit(Ctl *ctl, int nstages)
 
 // ---- P -> U on interior zones (GodunovOperator::PrimToCons, Mara/hydro.cpp:112-123) ----------
 template <class T>
-__global__ void __launch_bounds__(256) k_prim_to_cons(Grid g, StateCPtr<T> P0, StateCPtr<T> P1, StatePtr<T> U,
-                                                      double gamma, const Ctl *ctl)
+__device__ __forceinline__ void p2c_zone(const Grid &g, StateCPtr<T> P, StatePtr<T> U, double gamma, long long t)
 {
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
   int i, j, k;
   interior_coords(g, t, i, j, k);
   const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-  const StateCPtr<T> P = ctl->cur ? P1 : P0;
   double p[8], u[8];
   load_state(g, P, z, p);
   prim_to_cons(gamma, p, u);
@@ -110,27 +112,25 @@ __global__ void __launch_bounds__(256) k_prim_to_cons(Grid g, StateCPtr<T> P0, S
   for (int c = 0; c < 3; ++c) U.B[c * g.cs + z] = u[5 + c];
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) k_prim_to_cons(Grid g, StateCPtr<T> P0, StateCPtr<T> P1, StatePtr<T> U,
+                                                      double gamma, const Ctl *ctl)
+{
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  p2c_zone<T>(g, ctl->cur ? P1 : P0, U, gamma, t);
+}
+
 // ---- c2p with guard scatter (GodunovOperator::ConsToPrim, Mara/hydro.cpp:125-202) -----------
 // Stage c2p (final == 0): guess from PA (or zeros on the first stage, as the reference's
 // PrimitiveArray is zero-filled by every advance, Mara/mara.cpp:321); result into PA.
 // Closing c2p (final == 1): guess from PA, result into the next committed state.
+// Counts a zone's c2p outcome and scatters its primitives to the zone and its guard images.
 template <class T>
-__global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
-                                                      PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
-                                                      int ereset, double preset, double dreset)
+__device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn, Ctl *ctl, int stage, int final,
+                                           int ereset, double preset, double dreset, int i, int j, int k,
+                                           const double *u, double *p, int err, const C2PTally &tally)
 {
-  if (stage_failed(ctl, stage)) return;
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
-  int i, j, k;
-  interior_coords(g, t, i, j, k);
-  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-  double u[8], p[8];
-  load_state(g, U, z, u);
-#pragma unroll
-  for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
-  C2PTally tally;
-  int err = cons_to_prim(pp, u, p, &tally) != 0;
   warp_add(&ctl->c2p_calls, 1u);
   warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
   if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
@@ -150,7 +150,6 @@ __global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T 
   const int ni = images_1d(i, g.n[0], g.ng, g.nd >= 1, pi);
   const int nj = images_1d(j, g.n[1], g.ng, g.nd >= 2, pj);
   const int nk = images_1d(k, g.n[2], g.ng, g.nd >= 3, pk);
-  StatePtr<T> Pn = ctl->cur ? Pn0 : Pn1;   // the buffer that is not committed
   for (int a = 0; a < ni; ++a)
     for (int b = 0; b < nj; ++b)
       for (int c = 0; c < nk; ++c) {
@@ -167,81 +166,117 @@ __global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T 
       }
 }
 
+// One interior zone's c2p (per-thread path, optional per-thread network guess).
+template <class T>
+__device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, StatePtr<T> Pn, const PhysParams &pp,
+                                         Ctl *ctl, int stage, int zero_guess, int final, int ereset, double preset,
+                                         double dreset, long long t)
+{
+  int i, j, k;
+  interior_coords(g, t, i, j, k);
+  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+  double u[8], p[8];
+  load_state(g, U, z, u);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+  C2PTally tally;
+  const int err = cons_to_prim<(sizeof(T) < sizeof(double))>(pp, u, p, &tally) != 0;
+  c2p_finish<T>(g, PA, Pn, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err, tally);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
+                                                      PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
+                                                      int ereset, double preset, double dreset)
+{
+  if (stage_failed(ctl, stage)) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  c2p_zone<T>(g, U, PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, t);
+}
+
 // ---- flux sweep (MethodOfLinesSplit::intercell_flux_sweep, Mara/plm-split.cpp:43-73) ---------
 // One thread per face.  The face set is the reference's: every zone index f with
 // 2*S <= f < nz - 3*S in the flattened guarded array (S the zone stride of `dim`), the face
 // between zones f and f + S.  Faces that straddle a row end in the flattened array are
 // evaluated too, because they enter MaxLambda in the reference.
-template <class T>
-__global__ void __launch_bounds__(128) k_flux(Grid g, int dim, const T *__restrict__ PA, T *__restrict__ F,
-                                              PhysParams pp, Ctl *ctl, int stage)
+// Per-thread flux statistics, summed per block.
+struct FluxTally {
+  int hlld_ok, hlld_hllc, pcm_retry, face_c2p_calls, face_c2p_iters;
+};
+
+// One face: reconstruct, Riemann solve (PCM retry on failure), store the flux; the face's
+// |lambda| is folded into ml.
+template <class T, int dim>
+__device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ PA, T *__restrict__ F,
+                                          const PhysParams &pp, long long f, T &ml, FluxTally &ft)
 {
-  if (stage_failed(ctl, stage + 1)) return;
   const long long S = g.s[dim - 1];
-  const long long f = 2 * S + (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  T ml = T(0);
-  int used_hllc = 0, pcm_retry = 0, hlld = 0;
-  C2PTally tally{0, 0};
-  if (f < g.nz - 3 * S) {
-    T Pl[8], Pr[8];
-    const T theta = T(pp.theta);
+  T Pl[8], Pr[8];
+  const T theta = T(pp.theta);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const T *a = PA + q * g.cs + f;
-      if (pp.recon == RECON_PCM) {
-        Pl[q] = a[0];
-        Pr[q] = a[S];
-      } else if (pp.recon == RECON_PLM) {
-        const T vm = a[-S], v0 = a[0], vp = a[S], vpp = a[2 * S];
-        Pl[q] = plm(theta, vm, v0, vp, T(+1));
-        Pr[q] = plm(theta, v0, vp, vpp, T(-1));
-      } else {
-        const T vm2 = a[-2 * S], vm1 = a[-S], v0 = a[0], vp1 = a[S], vp2 = a[2 * S], vp3 = a[3 * S];
-        Pl[q] = weno5(pp.is_mode, T(pp.sz10A), vm2, vm1, v0, vp1, vp2, true);
-        Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
-      }
-    }
-    T Fo[8];
-    const T gamma = T(pp.gamma);
-    int err;
-    if (pp.riemann == RIEMANN_HLLD) {
-      hlld = 1;
-      err = riemann_hlld<T>(pp, Pl, Pr, Fo, dim, ml, used_hllc, &tally);
-    } else if (pp.riemann == RIEMANN_HLLC) {
-      err = riemann_hllc<T>(gamma, Pl, Pr, Fo, dim, ml);
+  for (int q = 0; q < 8; ++q) {
+    const T *a = PA + q * g.cs + f;
+    if (pp.recon == RECON_PCM) {
+      Pl[q] = a[0];
+      Pr[q] = a[S];
+    } else if (pp.recon == RECON_PLM) {
+      const T vm = a[-S], v0 = a[0], vp = a[S], vpp = a[2 * S];
+      Pl[q] = plm(theta, vm, v0, vp, T(+1));
+      Pr[q] = plm(theta, v0, vp, vpp, T(-1));
     } else {
-      err = riemann_hll<T>(gamma, Pl, Pr, Fo, dim, ml);
+      const T vm2 = a[-2 * S], vm1 = a[-S], v0 = a[0], vp1 = a[S], vp2 = a[2 * S], vp3 = a[3 * S];
+      Pl[q] = weno5(pp.is_mode, T(pp.sz10A), vm2, vm1, v0, vp1, vp2, true);
+      Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
     }
-    if (err) {   // retry with the zone states themselves (PCM)
-      pcm_retry = 1;
-      T tally_iters = 0;
-      (void) tally_iters;
+  }
+  T Fo[8];
+  const T gamma = T(pp.gamma);
+  int err = 1, used_hllc = 0;
+  const bool hlld = pp.riemann == RIEMANN_HLLD;
+  C2PTally tally{0, 0};
+  // attempt 0: reconstructed states; attempt 1: the zone states themselves (PCM retry).
+  // One call site per solver keeps a single inlined copy of it.
+#pragma unroll 1
+  for (int attempt = 0; attempt < 2 && err; ++attempt) {
+    if (attempt == 1) {
+      ft.pcm_retry += 1;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         Pl[q] = PA[q * g.cs + f];
         Pr[q] = PA[q * g.cs + f + S];
       }
-      C2PTally t2{0, 0};
-      if (pp.riemann == RIEMANN_HLLD) err = riemann_hlld<T>(pp, Pl, Pr, Fo, dim, ml, used_hllc, &t2);
-      else if (pp.riemann == RIEMANN_HLLC) err = riemann_hllc<T>(gamma, Pl, Pr, Fo, dim, ml);
-      else err = riemann_hll<T>(gamma, Pl, Pr, Fo, dim, ml);
-      tally.iters += t2.iters;
-      tally.attempts += t2.attempts;
-      if (err) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) Fo[q] = T(0);
-      }
     }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
+    C2PTally t{0, 0};
+    if (hlld) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
+    else if (pp.riemann == RIEMANN_HLLC) err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
+    else err = riemann_hll<T, dim>(gamma, Pl, Pr, Fo, ml);
+    tally.iters += t.iters;
+    tally.attempts += t.attempts;
   }
-  // MaxLambda: warp max -> block max -> one atomic per block (non-negative doubles order
-  // like their bit patterns)
-  double m = double(ml);
+  if (err) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) Fo[q] = T(0);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
+  if (hlld) {
+    ft.hlld_ok += 1 - used_hllc;
+    ft.hlld_hllc += used_hllc;
+  }
+  ft.face_c2p_calls += tally.attempts > 0;
+  ft.face_c2p_iters += tally.iters;
+}
+
+// MaxLambda of a block: warp max -> block max -> one atomicMax (non-negative doubles order
+// like their bit patterns); plus the block's flux statistics.  All threads must call.
+__device__ __forceinline__ void flux_block_finish(double m, const FluxTally &ft, Ctl *ctl, bool hlld)
+{
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   __shared__ double wmax[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();   // wmax may still be read from a previous tile
   if (lane == 0) wmax[warp] = m;
   __syncthreads();
   if (warp == 0) {
@@ -251,12 +286,25 @@ __global__ void __launch_bounds__(128) k_flux(Grid g, int dim, const T *__restri
     if (lane == 0 && m > 0.0) atomicMax(&ctl->max_lambda_bits, (unsigned long long) __double_as_longlong(m));
   }
   if (hlld) {
-    warp_add(&ctl->hlld_ok, (unsigned) (1 - used_hllc));
-    warp_add(&ctl->hlld_hllc, (unsigned) used_hllc);
+    warp_add(&ctl->hlld_ok, (unsigned) ft.hlld_ok);
+    warp_add(&ctl->hlld_hllc, (unsigned) ft.hlld_hllc);
   }
-  warp_add(&ctl->pcm_retry, (unsigned) pcm_retry);
-  warp_add(&ctl->face_c2p_calls, (unsigned) (tally.attempts > 0));
-  warp_add(&ctl->face_c2p_iters, (unsigned) tally.iters);
+  warp_add(&ctl->pcm_retry, (unsigned) ft.pcm_retry);
+  warp_add(&ctl->face_c2p_calls, (unsigned) ft.face_c2p_calls);
+  warp_add(&ctl->face_c2p_iters, (unsigned) ft.face_c2p_iters);
+}
+
+template <class T, int dim>
+__global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_flux(Grid g, const T *__restrict__ PA, T *__restrict__ F,
+                                                              PhysParams pp, Ctl *ctl, int stage)
+{
+  if (stage_failed(ctl, stage + 1)) return;
+  const long long S = g.s[dim - 1];
+  const long long f = 2 * S + (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  T ml = T(0);
+  FluxTally ft{0, 0, 0, 0, 0};
+  if (f < g.nz - 3 * S) flux_face<T, dim>(g, PA, F, pp, f, ml, ft);
+  flux_block_finish(double(ml), ft, ctl, pp.riemann == RIEMANN_HLLD);
 }
 
 // ---- CT + flux divergence + Runge-Kutta combine ---------------------------------------------
@@ -301,21 +349,17 @@ __device__ __forceinline__ T combine_bulk(const UpdateArgs &a, T un, T us, T dt,
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
-                                                const T *__restrict__ F, const T *__restrict__ G,
-                                                const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
-                                                StateCPtr<T> K1, StateCPtr<T> K2, StateCPtr<T> K3,
-                                                const Ctl *ctl, int stage)
+__device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, StateCPtr<T> Un, StateCPtr<T> Us,
+                                            const T *__restrict__ F, const T *__restrict__ G,
+                                            const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
+                                            StateCPtr<T> K1, StateCPtr<T> K2, StateCPtr<T> K3, double dtd,
+                                            long long t)
 {
-  if (stage_failed(ctl, stage + 1)) return;
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
   int i, j, k;
   interior_coords(g, t, i, j, k);
   const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
   const long long sx = g.s[0], sy = g.s[1], sz = g.s[2];
   const double dx = g.dx, dy = g.dy, dz = g.dz;
-  const double dtd = ctl->dt;
   const T dt = T(dtd);
   const bool rk4 = a.combine >= COMB_RK4_K;
   // bulk components 0..4: plain flux differences in T
@@ -377,6 +421,19 @@ __global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<
     }
     Uout.B[c * g.cs + z] = out;
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
+                                                const T *__restrict__ F, const T *__restrict__ G,
+                                                const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
+                                                StateCPtr<T> K1, StateCPtr<T> K2, StateCPtr<T> K3,
+                                                const Ctl *ctl, int stage)
+{
+  if (stage_failed(ctl, stage + 1)) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  update_zone<T>(g, a, Un, Us, F, G, H, Uout, Kout, K1, K2, K3, ctl->dt, t);
 }
 
 }  // namespace mgpu

@@ -1,0 +1,96 @@
+// The zone c2p kernel with the learned initial guess evaluated on the tensor cores.
+//
+// Persistent: each CTA sets up the network image, TMEM and its mbarrier once, then walks
+// tiles of 128 interior zones.  Per tile the 128 threads stage their zones' features, the
+// CTA runs the four MMA layers (c2p_mlp_tc.cuh), and each thread polishes its own zone with
+// the FP64 Newton iteration from the network's (Z, W) -- the reference's ladder follows when
+// that attempt fails -- then scatters the primitives to the zone's guard images, exactly as
+// k_cons_to_prim does.
+#pragma once
+#include "c2p_mlp_tc.cuh"
+#include "rmhd_step.cuh"
+
+namespace mgpu {
+
+template <class T>
+__global__ void __launch_bounds__(128) k_cons_to_prim_tc(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
+                                                         StatePtr<T> Pn1, PhysParams pp, Ctl *ctl, int stage,
+                                                         int zero_guess, int final, int ereset, double preset,
+                                                         double dreset)
+{
+  if (stage_failed(ctl, stage)) return;
+  extern __shared__ unsigned char tc_smem[];
+  tc::TcNet net = tc::tc_setup(tc_smem, (const unsigned char *) pp.mlp_tc);
+  const long long ntiles = (g.ninterior + 127) / 128;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long t = tile * 128 + threadIdx.x;
+    const bool valid = t < g.ninterior;
+    int i = 0, j = 0, k = 0;
+    long long z = 0;
+    double u[8], p[8];
+    float xn[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    bool good = false;
+    if (valid) {
+      interior_coords(g, t, i, j, k);
+      z = ((long long) i * g.G[1] + j) * g.G[2] + k;
+      load_state(g, U, z, u);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+      if (check_cons(u) == C2P_SUCCESS) {
+        const double S2 = u[Sx] * u[Sx] + u[Sy] * u[Sy] + u[Sz] * u[Sz];
+        const double B2 = u[Bx] * u[Bx] + u[By] * u[By] + u[Bz] * u[Bz];
+        const double BS = u[Bx] * u[Sx] + u[By] * u[Sy] + u[Bz] * u[Sz];
+        float x[5];
+        c2p_features(u[ddd], u[tau], S2, B2, BS * BS, x);
+        net.normalise(x, xn);
+        good = isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]) && isfinite(xn[3]) && isfinite(xn[4]);
+        if (!good) xn[0] = xn[1] = xn[2] = xn[3] = xn[4] = 0.f;
+      }
+    }
+    float y[2];
+    const bool have = net.forward(xn, y);
+    if (!valid) continue;
+    double Zg = 0.0, Wg = 0.0;
+    const bool use = have && good && c2p_guess_from_output(u[ddd], y, Zg, Wg);
+    C2PTally tally;
+    int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
+    warp_add(&ctl->c2p_calls, 1u);
+    warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
+    if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
+    if (err) {
+      if (ereset) {
+        p[0] = dreset;
+        p[1] = preset;
+        p[2] = p[3] = p[4] = 0.0;
+        p[5] = u[5];
+        p[6] = u[6];
+        p[7] = u[7];
+      } else {
+        atomicAdd(final ? &ctl->final_err : &ctl->stage_err[stage], multiplicity(g, i, j, k));
+      }
+    }
+    int pi[3], pj[3], pk[3];
+    const int ni = images_1d(i, g.n[0], g.ng, g.nd >= 1, pi);
+    const int nj = images_1d(j, g.n[1], g.ng, g.nd >= 2, pj);
+    const int nk = images_1d(k, g.n[2], g.ng, g.nd >= 3, pk);
+    StatePtr<T> Pn = ctl->cur ? Pn0 : Pn1;
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b)
+        for (int c = 0; c < nk; ++c) {
+          const long long w = ((long long) pi[a] * g.G[1] + pj[b]) * g.G[2] + pk[c];
+          if (final) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) Pn.bulk[q * g.cs + w] = T(p[q]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) Pn.B[q * g.cs + w] = p[5 + q];
+          } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) PA[q * g.cs + w] = T(p[q]);
+          }
+        }
+  }
+  if (!net.ok && threadIdx.x == 0) atomicExch(&ctl->tc_fault, 1);
+  tc::tc_teardown(net);
+}
+
+}  // namespace mgpu

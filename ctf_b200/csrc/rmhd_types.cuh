@@ -27,8 +27,10 @@ struct PhysParams {
   int is_mode;       // reconstruct_set_smoothness_indicator
   int recon;         // GodunovOperator::reconstruct_method
   int riemann;
-  int learned;       // learned c2p initial guess on/off
-  const void *mlp;   // device pointer to the packed c2p network (nullptr when off)
+  int learned;       // learned c2p initial guess on/off (zone c2p)
+  int learned_faces; // also for the HLL-state c2p inside HLLD (per-thread evaluation)
+  const void *mlp;   // device pointer to the packed FP32 c2p network (nullptr when off)
+  const void *mlp_tc;// device pointer to its tensor-core image (nullptr: per-thread path)
 };
 
 constexpr int MAX_STAGES = 4;
@@ -41,7 +43,7 @@ struct Ctl {
   int final_err;                        // failures of the closing c2p
   int cur;                              // committed primitive buffer (0/1)
   int committed;                        // 1 if the last advance was committed
-  int pad;
+  int tc_fault;                         // a tensor-core wait timed out (sticky)
   // statistics, accumulated over the advance
   unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
   unsigned long long face_c2p_calls, face_c2p_iters;

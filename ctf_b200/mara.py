@@ -191,6 +191,12 @@ class Solver:
         self._check(self.lib.mgpu_measure_divB(self.h, ctypes.byref(m), ctypes.byref(x)))
         return m.value, x.value
 
+    def mean_max_divB_state(self):
+        """Corner divergence of the committed state's (FP64) magnetic field."""
+        m, x = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mgpu_measure_divB_state(self.h, ctypes.byref(m), ctypes.byref(x)))
+        return m.value, x.value
+
     def max_lorentz_factor(self) -> float:
         w = ctypes.c_double()
         self._check(self.lib.mgpu_max_lorentz_factor(self.h, ctypes.byref(w)))

@@ -113,6 +113,9 @@ int mgpu_set_primitive(mgpu_solver *h, const double *host_aos);
  * reference, or the array given to mgpu_set_primitive). */
 int mgpu_measure_divB(mgpu_solver *h, double *mean, double *max);
 int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax);
+/* The same corner divergence on the committed state, whose magnetic field is FP64 in both
+ * precisions (the FP32-bulk path keeps B, its CT update and ∇·B in FP64). */
+int mgpu_measure_divB_state(mgpu_solver *h, double *mean, double *max);
 
 /* Kernel timing (no counterpart in the reference): while enabled, every kernel launch of an
  * advance is bracketed by CUDA events on the handle's stream.  Classes: 0 begin/commit,
@@ -123,9 +126,34 @@ int mgpu_profile_enable(mgpu_solver *h, int capacity);
 int mgpu_profile_disable(mgpu_solver *h);
 int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long *units);
 
-/* Learned c2p initial guess: weights of the packed network (layout in ctf_b200/csrc/
- * c2p_mlp_net.cuh), copied to the device.  No counterpart in the reference. */
+/* Learned c2p initial guess (no counterpart in the reference).  A 5 -> 64 -> 64 -> 64 -> 2
+ * tanh network maps scale-free features of the c2p invariants (D, tau, S^2, B^2, (S.B)^2)
+ * to (log W, log h); the FP64 Newton polish starts there and the reference's ladder runs if
+ * it fails.  Packed float32 parameters (mgpu_mlp_param_count of them; layout in
+ * ctf_b200/csrc/c2p_mlp_net.cuh).  All pointers named dev_* are device pointers. */
 int mgpu_set_c2p_network(mgpu_solver *h, const float *params, long long count);
+int mgpu_mlp_param_count(void);
+/* (features, targets) of every interior zone of the committed state: n = interior zones,
+ * dev_x n x 5 floats, dev_y n x 2 floats (log W, log h). */
+int mgpu_c2p_harvest(mgpu_solver *h, float *dev_x, float *dev_y, long long capacity, long long *count);
+/* Scratch for mgpu_mlp_loss_grad / mgpu_mlp_train over `batch` samples, in floats. */
+long long mgpu_mlp_work_floats(long long batch);
+/* Mean squared error of the standardised outputs over n samples and its gradient with
+ * respect to the trainable parameters (deterministic order). */
+int mgpu_mlp_loss_grad(const float *dev_params, const float *dev_x, const float *dev_y, long long n,
+                       float *dev_grad, float *dev_work, double *loss);
+/* `steps` minibatch Adam steps (batch samples each, learning rate lr; step0 = steps taken
+ * before, for the bias corrections and the data walk); *last_loss = last minibatch loss. */
+int mgpu_mlp_train(float *dev_params, float *dev_m, float *dev_v, const float *dev_x, const float *dev_y,
+                   long long n, int batch, int steps, float lr, int step0, float *dev_work, double *last_loss);
+/* The network on n feature rows (dev_x n x 5) -> dev_y n x 2 (log W, log h). */
+int mgpu_mlp_forward(const float *dev_params, const float *dev_x, long long n, float *dev_y);
+/* The same on the tensor cores (BF16 weights and activations, FP32 accumulation), from the
+ * host-side FP32 parameters: the path the zone c2p kernel uses when a network is set. */
+int mgpu_mlp_forward_tc(const float *params, const float *dev_x, long long n, float *dev_y);
+/* The tensor-core image of a network (mgpu_mlp_tc_image_bytes bytes, host memory). */
+int mgpu_mlp_tc_image_bytes(void);
+int mgpu_mlp_build_tc_image(const float *params, void *image);
 
 /* Allocation-free advance (no counterpart in the reference).  For callers that may not
  * allocate device memory -- allocation-free sections of a larger application, real-time

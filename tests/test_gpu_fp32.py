@@ -1,0 +1,104 @@
+"""The FP32-bulk path against the plain FP64 path (it has no reference oracle of its own).
+
+FP32 carries reconstruction, the Riemann fluxes and the RK combine of rho, tau, S; FP64
+carries the c2p Newton polish, the magnetic field with its constrained-transport update,
+and the dt reduction.  Both paths advance the same box with the same fixed dt; the stated
+bounds are the per-field relative L1 and L-infinity differences after the steps, and the
+corner divergence of the FP32 path's (FP64) magnetic field.
+"""
+import numpy as np
+import pytest
+
+from ctf_b200 import ics
+from ctf_b200.mara import Scheme, Solver
+
+pytestmark = pytest.mark.gpu
+
+L1_TOL = 1e-5          # relative L1 per field (north-star density bound, applied to every field)
+LINF_TOL = 5e-3        # relative L-infinity per field (FP32 rounding at discontinuities)
+DIVB_TOL = 1e-12       # corner divergence of B (as Mara.measure.mean_max_divB reports it)
+
+
+def interior(P, nd, ng=3):
+    return P[tuple(slice(ng, -ng) if d < nd else slice(None) for d in range(3))]
+
+
+def rel_errors(a, b, nd):
+    a, b = interior(a, nd).reshape(-1, 8), interior(b, nd).reshape(-1, 8)
+    l1, linf = [], []
+    for q in range(8):
+        s1, sinf = np.abs(b[:, q]).mean(), np.abs(b[:, q]).max()
+        d = np.abs(a[:, q] - b[:, q])
+        l1.append(d.mean() / s1 if s1 > 0 else d.mean())
+        linf.append(d.max() / sinf if sinf > 0 else d.max())
+    return np.array(l1), np.array(linf)
+
+
+def run(prec, kw, n, P0, dt, steps):
+    s = Solver(Scheme(precision=prec, **kw), n, None, None)
+    s.upload(P0.copy())
+    for _ in range(steps):
+        assert s.advance(dt) == 0
+    return s
+
+
+@pytest.mark.parametrize("kw,n,steps,vrms", [
+    (dict(extrap="plm", riemann="hlld", advance="rk2"), (32, 32, 32), 20, 0.3),
+    (dict(extrap="weno5", riemann="hlld", advance="rk3"), (32, 32, 32), 10, 0.3),
+    # HLLC on these boxes fails c2p within a few steps in the reference itself (the
+    # step_hllc_fail_12 fixture; at 0.15c the bit-exact restatement fails at step 7), so
+    # this case stops after 6 steps of a gentler box
+    (dict(extrap="plm", riemann="hllc", advance="rk3"), (24, 20, 16), 6, 0.15),
+])
+def test_fp32_bulk_tracks_fp64_turbulence(kw, n, steps, vrms):
+    P0 = ics.turbulence_box(n, seed=31, vrms=vrms)
+    ref = Solver(Scheme(**kw), n)
+    ref.upload(P0.copy())
+    assert ref.advance(0.0) == 0
+    dt = ref.get_timestep(0.3)
+    a = run("fp32", kw, n, P0, dt, steps)
+    b = run("fp64", kw, n, P0, dt, steps)
+    l1, linf = rel_errors(a.download(), b.download(), 3)
+    assert l1.max() <= L1_TOL, l1
+    assert linf.max() <= LINF_TOL, linf
+    mean, mx = a.mean_max_divB_state()
+    assert abs(mx) <= DIVB_TOL and abs(mean) <= DIVB_TOL
+
+
+def test_fp32_bulk_kelvin_helmholtz_2d():
+    kw = dict(extrap="plm", riemann="hllc", advance="rk3")
+    n = (64, 64)
+    P0 = ics.kh_box(n, seed=32)
+    ref = Solver(Scheme(**kw), n)
+    ref.upload(P0.copy())
+    assert ref.advance(0.0) == 0
+    dt = ref.get_timestep(0.3)
+    a = run("fp32", kw, n, P0, dt, 20)
+    b = run("fp64", kw, n, P0, dt, 20)
+    A, B = interior(a.download(), 2).reshape(-1, 8), interior(b.download(), 2).reshape(-1, 8)
+    # rho and p relative to themselves; v and B components relative to the mean |v| and
+    # |B| (vy and By start as small perturbations of a flow along x)
+    vs = np.sqrt((B[:, 2:5] ** 2).sum(1)).mean()
+    bs = np.sqrt((B[:, 5:8] ** 2).sum(1)).mean()
+    scale = np.array([np.abs(B[:, 0]).mean(), np.abs(B[:, 1]).mean(), vs, vs, vs, bs, bs, bs])
+    l1 = np.abs(A - B).mean(0) / scale
+    assert l1.max() <= L1_TOL, l1
+    assert abs(a.mean_max_divB_state()[1]) <= DIVB_TOL
+
+
+def test_fp32_device_dt_loop_matches_host_loop():
+    """advance_async with the device-side dt (cfl * min_dx / MaxLambda of the previous
+    step) follows the same sequence as a host loop of get_timestep + advance."""
+    kw = dict(extrap="plm", riemann="hlld", advance="rk2", precision="fp32")
+    n = (16, 16, 16)
+    P0 = ics.turbulence_box(n, seed=33)
+    a = Solver(Scheme(**kw), n)
+    b = Solver(Scheme(**kw), n)
+    for s in (a, b):
+        s.upload(P0.copy())
+        assert s.advance(0.0) == 0
+    for _ in range(5):
+        assert b.advance(b.get_timestep(0.3)) == 0
+    a.advance_async(5, cfl=0.3)
+    a.synchronize()
+    assert np.array_equal(a.download(), b.download())

@@ -19,6 +19,7 @@ advances its own box: independent replicas, weak scaling, no collective on the d
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -46,6 +47,11 @@ WORKLOADS = {
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
 }
 DEFAULT_WORKLOAD = "turb256_weno5_hlld_rk3"
+# ensembles: 256 independent 2D Kelvin-Helmholtz boxes, sides log-uniform in 64..512
+ENSEMBLE_WORKLOADS = {
+    "kh_ensemble256_plm_hllc_rk3": dict(nboxes=256, lo=64, hi=512,
+                                        scheme=dict(extrap="plm", riemann="hllc", advance="rk3")),
+}
 CFL = 0.3
 
 
@@ -171,10 +177,206 @@ def _cpu_worker(args):
     return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed)
 
 
+def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0):
+    """The reference's CPU advance of one 2D Kelvin-Helmholtz box (bounded sample)."""
+    from ctf_b200 import ics
+    from oracle import PortOracle, REF_SO, RefOracle, Scheme
+    sch = Scheme(n=(n, n), **scheme_kw)
+    kind = "reference" if os.path.exists(REF_SO) else "port"
+    o = RefOracle(sch) if kind == "reference" else PortOracle(sch)
+    P = np.ascontiguousarray(ics.kh_box((n, n), seed=seed))
+    o.advance(P, 0.0)
+    dt = o.get_timestep(CFL)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.advance(P, dt)
+    sec = time.perf_counter() - t0
+    if kind == "reference":
+        o.close()
+    return kind, n * n * steps / sec, sec
+
+
+def _cpu_worker_kh(args):
+    scheme_kw, steps, n, seed = args
+    return cpu_sample_kh(scheme_kw, steps=steps, n=n, seed=seed)
+
+
+def run_ensemble_bench(args, rank, world, local):
+    """An ensemble of independent 2D KH boxes advanced as one CUDA graph per step (FP32 bulk,
+    autotuned launch shape), with the FP64 ensemble of the same boxes and dt beside it."""
+    import torch
+    from ctf_b200 import ics
+    from ctf_b200.ensemble import Ensemble, kh_sizes
+    from ctf_b200.mara import Scheme
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    wl = ENSEMBLE_WORKLOADS[args.workload]
+    kw = wl["scheme"]
+    sizes = kh_sizes(wl["nboxes"], seed=rank, lo=wl["lo"], hi=wl["hi"])
+    states = [np.ascontiguousarray(ics.kh_box(n, seed=1000 * rank + b)) for b, n in enumerate(sizes)]
+    zones = sum(a * b for a, b in sizes)
+    stream = torch.cuda.Stream()
+
+    def make(prec):
+        E = Ensemble(Scheme(precision=prec, **kw), sizes)
+        E.set_stream(stream.cuda_stream)
+        for b, P in enumerate(states):
+            E.upload(b, P)
+        E.advance(dt=0.0)
+        return E
+
+    def timed(E, dt):
+        E.advance(dt=dt, nsteps=1)   # capture the one-step graph
+        for _ in range(args.warmup - 1):
+            E.advance(dt=dt, nsteps=1)
+        E.synchronize()
+        if dist is not None:
+            dist.barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            start.record(stream)
+            for _ in range(args.steps):
+                E.advance(dt=dt, nsteps=1)
+            end.record(stream)
+            end.synchronize()
+        ms = start.elapsed_time(end)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        assert not E.errors().any(), "an ensemble box failed"
+        return ms, clk.summary()
+
+    out_runs, finals = {}, {}
+    dt = None
+    for prec in (["fp64"] if not args.skip_fp64 else []) + ["fp32"]:
+        E = make(prec)
+        if dt is None:
+            dt = E.timesteps(CFL)
+        tune = None
+        if prec == "fp32":
+            shape, tms = E.autotune(dt, reps=2)
+            tune = {"launch": shape, "ms_per_step": tms}
+        ms, clk = timed(E, dt)
+        finals[prec] = [E.download(b) for b in range(E.nb)]
+        # kernel shares from one direct (profiled) advance of the same state
+        E.profile_enable(256)
+        E.advance(dt=dt, nsteps=1, graph=False)
+        prof = E.profile_read()
+        E.profile_disable()
+        out_runs[prec] = {"value": zones * args.steps * world / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                          "clocks": clk, "prof": prof, "tuning": tune, "ensemble": E}
+        if prec == "fp64":
+            E.close()
+    head = out_runs["fp32"]
+    E = head["ensemble"]
+    prof = head["prof"]
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    dom = max(("flux", "update", "c2p", "p2c"), key=lambda k: prof[k]["ms"])
+    per_unit = {"flux": 16 * 4, "update": 5 * 4 * 3 + 3 * 8 * 3 + 2 * 8 * 4, "c2p": 44 + 8 * 4, "p2c": 88}
+    d = prof[dom]
+    achieved = per_unit[dom] * d["units"] / (d["ms"] * 1e-3) / 1e9
+    line = {
+        "metric": "RMHD zone-updates/s on 1 B200: ensemble of 256 uneven 2D KH boxes, FP32 bulk, one graph per step",
+        "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "boxes": wl["nboxes"], "sides": [wl["lo"], wl["hi"]],
+                   "interior_zones": zones, "scheme": kw, "cfl": CFL,
+                   "dt": "per box, CFL 0.3 of its primed MaxLambda (same for both precisions)",
+                   "l2": "all boxes' arrays together (~4 GB) > 126 MB L2 (no flush needed)",
+                   "launch": head["tuning"]["launch"], "tuned_ms_per_step": head["tuning"]["ms_per_step"]},
+        "gpu_launches": (2 + 3 * 4 + 2) * args.steps,
+        "clocks": head["clocks"],
+        "runs": {k: {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                     "kernel_ms_per_step": {c: r["prof"][c]["ms"] for c in r["prof"]}}
+                 for k, r in out_runs.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes_per_unit": per_unit[dom]},
+    }
+    if "fp64" in finals:
+        line["speedup_vs_fp64"] = head["value"] / out_runs["fp64"]["value"]
+        num = np.zeros(8)
+        den = np.zeros(8)
+        for a, b in zip(finals["fp32"], finals["fp64"]):
+            a, b = a[3:-3, 3:-3].reshape(-1, 8), b[3:-3, 3:-3].reshape(-1, 8)
+            num += np.abs(a - b).sum(0)
+            den += np.abs(b).sum(0)
+        names = ["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]
+        line["l1_rel_vs_fp64"] = {n: float(num[q] / den[q]) if den[q] > 0 else float(num[q])
+                                  for q, n in enumerate(names)}
+    if not args.no_e2e:
+        hosts = []
+        for b, P in enumerate(states):
+            h = torch.empty(P.shape, dtype=torch.float64, pin_memory=True).numpy()
+            h[...] = E.download(b)
+            hosts.append(h)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for b in range(E.nb):
+                E.lib.mgpu_ensemble_upload_prim(E.h, b, hosts[b].ctypes.data_as(
+                    ctypes.POINTER(ctypes.c_double)))
+            E.advance(dt=dt, nsteps=1)
+            errs = E.errors()
+            for b in range(E.nb):
+                E.lib.mgpu_ensemble_download_prim(E.h, b, hosts[b].ctypes.data_as(
+                    ctypes.POINTER(ctypes.c_double)))
+        sec = time.perf_counter() - t0
+        assert not errs.any()
+        nbytes = sum(h.nbytes for h in hosts)
+        line["e2e"] = {"value": zones * args.steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                       "d2h_bytes_per_step": nbytes,
+                       "api": "mgpu_ensemble_upload_prim + mgpu_ensemble_advance + mgpu_ensemble_download_prim"}
+    E.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, v, sec = cpu_sample_kh(kw, steps=2, n=256)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                                "sample": f"one 256^2 KH box, same scheme, 2 steps after priming ({sec:.1f} s), "
+                                          "interior zone-updates/s on 1 core"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args, wl_name, rank, world):
     """--impl reference: the reference's own CPU advance on every host core (independent
-    replicas of a 64^3 sample box of the workload's scheme)."""
+    replicas of a 64^3 sample box of the workload's scheme, or 256^2 KH boxes for an
+    ensemble workload)."""
     if rank != 0:
+        return
+    if wl_name in ENSEMBLE_WORKLOADS:
+        import multiprocessing as mp
+        kw = ENSEMBLE_WORKLOADS[wl_name]["scheme"]
+        cores = os.cpu_count() or 1
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cpu_worker_kh, [(kw, args.steps, 256, s) for s in range(cores)])
+        wall = time.perf_counter() - t0
+        value = float(sum(r[1] for r in res))
+        line = {"metric": "RMHD zone-updates/s on 1 B200: ensemble of 256 uneven 2D KH boxes, FP32 bulk, "
+                          "one graph per step", "value": value, "unit": UNIT, "impl": "reference",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": float(np.mean([r[2] for r in res]) / args.steps * 1e3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": wl_name, "sample": f"{cores} replicas of a 256^2 KH box"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": res[0][0],
+                                 "sample": f"{cores} concurrent 256^2 KH boxes x {args.steps} steps; wall {wall:.1f} s"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     n_wl, _, scheme_kw = WORKLOADS[wl_name]
     import multiprocessing as mp
@@ -208,7 +410,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(ENSEMBLE_WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -222,6 +424,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, args.workload, rank, world)
+        return
+    if args.workload in ENSEMBLE_WORKLOADS:
+        run_ensemble_bench(args, rank, world, local)
         return
 
     import torch

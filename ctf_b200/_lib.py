@@ -40,6 +40,14 @@ class MgpuStats(ctypes.Structure):
         return d
 
 
+class MgpuEnsembleLaunch(ctypes.Structure):
+    _fields_ = [("zone_tile", ctypes.c_int), ("face_tile", ctypes.c_int), ("zone_ctas_per_sm", ctypes.c_int),
+                ("face_ctas_per_sm", ctypes.c_int), ("c2p_ctas_per_sm", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # exported symbol -> (restype, argtypes)
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -84,6 +92,30 @@ SIGNATURES = {
     "mgpu_mlp_build_tc_image": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _vp]),
     "mgpu_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), _dp, _dp, _ip, ctypes.c_int, _vp, _vp,
                                             ctypes.c_double, _ip, _dp, _vp, ctypes.c_char_p, ctypes.c_int]),
+    "mgpu_ensemble_create": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), ctypes.c_int, ctypes.c_int, _ip, _dp, _dp,
+                                            ctypes.POINTER(_vp)]),
+    "mgpu_ensemble_destroy": (ctypes.c_int, [_vp]),
+    "mgpu_ensemble_last_error": (ctypes.c_char_p, [_vp]),
+    "mgpu_ensemble_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "mgpu_ensemble_num_zones": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_ensemble_total_interior": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_ensemble_upload_prim": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "mgpu_ensemble_download_prim": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "mgpu_ensemble_upload_prim_device": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "mgpu_ensemble_download_prim_device": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "mgpu_ensemble_get_launch": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuEnsembleLaunch)]),
+    "mgpu_ensemble_set_launch": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuEnsembleLaunch)]),
+    "mgpu_ensemble_advance": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int]),
+    "mgpu_ensemble_synchronize": (ctypes.c_int, [_vp]),
+    "mgpu_ensemble_errors": (ctypes.c_int, [_vp, _ip]),
+    "mgpu_ensemble_get_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(MgpuStats)]),
+    "mgpu_ensemble_get_timesteps": (ctypes.c_int, [_vp, ctypes.c_double, _dp]),
+    "mgpu_ensemble_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "mgpu_ensemble_profile_disable": (ctypes.c_int, [_vp]),
+    "mgpu_ensemble_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong),
+                                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_ensemble_time_advance": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuEnsembleLaunch), _dp, ctypes.c_int, _dp]),
+    "mgpu_ensemble_autotune": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.POINTER(MgpuEnsembleLaunch), _dp]),
 }
 
 

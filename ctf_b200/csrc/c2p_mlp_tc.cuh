@@ -6,7 +6,8 @@
 // ((r/8)*(K/8) + k/8)*128 + (r%8)*16 + (k%8)*2 bytes; LBO = 128 B between K-adjacent core
 // matrices, SBO = K*16 B between row groups).  Accumulators are FP32 in TMEM (64 columns);
 // each layer's epilogue reads its row with tcgen05.ld (32x32b), adds the bias, applies tanh
-// and writes the next layer's BF16 operand.  One thread issues the MMAs and commits them to an
+// (packed BF16 pairs) and writes the next layer's BF16 operand.  One thread issues the MMAs
+// and commits them to an
 // mbarrier; every wait on it is bounded and reports a timeout instead of hanging.
 //
 // Network image on the device (bytes, built by mgpu_set_c2p_network from the FP32 weights):
@@ -118,6 +119,15 @@ __device__ __forceinline__ void store_chunk(unsigned char *A, int r, int c, int 
   *reinterpret_cast<uint4 *>(A + canon_offset(r, 8 * c, K)) = q;
 }
 
+// tanh of two packed BF16 values (the PTX tanh.approx.bf16x2 instruction): the activations
+// are BF16 operands of the next layer anyway, so the activation is evaluated at that width.
+__device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x)
+{
+  uint32_t y;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+  return y;
+}
+
 // CTA-wide network evaluation context (one per CTA; all 128 threads call every method).
 struct TcNet {
   unsigned char *img;   // network image in shared memory
@@ -156,10 +166,12 @@ struct TcNet {
     for (int c0 = 0; c0 < 64; c0 += 16) {
       float v[16];
       tmem_ld16(row + (uint32_t) c0, v);
+      uint32_t h[8];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = tanhf(v[i] + bias[c0 + i]);
-      store_chunk(A, r, c0 / 8, 64, v);
-      store_chunk(A, r, c0 / 8 + 1, 64, v + 8);
+      for (int i = 0; i < 8; ++i)
+        h[i] = tanh_bf16x2(pack_bf16x2(v[2 * i] + bias[c0 + 2 * i], v[2 * i + 1] + bias[c0 + 2 * i + 1]));
+      *reinterpret_cast<uint4 *>(A + canon_offset(r, c0, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4 *>(A + canon_offset(r, c0 + 8, 64)) = make_uint4(h[4], h[5], h[6], h[7]);
     }
   }
 

@@ -7,6 +7,12 @@
 #else
 #define MGPU_FLUX_MINB 3
 #endif
+#ifdef MGPU_C2P_MINB_OVERRIDE
+#define MGPU_C2P_MINB MGPU_C2P_MINB_OVERRIDE
+#endif
+#ifdef MGPU_TC_CTAS_OVERRIDE
+#define MGPU_TC_CTAS_PER_SM MGPU_TC_CTAS_OVERRIDE
+#endif
 #include "c2p_mlp.cuh"
 #include "rmhd_launch.cuh"
 MGPU_DEFINE_PRECISION(fp64, double)

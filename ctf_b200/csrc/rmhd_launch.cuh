@@ -6,26 +6,11 @@
 #include "rmhd_step.cuh"
 #include "rmhd_step_tc.cuh"
 
-namespace mgpu {
+#ifndef MGPU_TC_CTAS_PER_SM
+#define MGPU_TC_CTAS_PER_SM 4
+#endif
 
-struct ProfScope {
-  LaunchProfiler *p;
-  cudaStream_t s;
-  int slot;
-  ProfScope(LaunchProfiler *p_, cudaStream_t s_, int tag, long long units) : p(p_), s(s_), slot(-1)
-  {
-    if (p && *p->count < p->capacity) {
-      slot = (*p->count)++;
-      p->tag[slot] = tag;
-      p->units[slot] = units;
-      cudaEventRecord(p->ev[2 * slot], s);
-    }
-  }
-  ~ProfScope()
-  {
-    if (slot >= 0) cudaEventRecord(p->ev[2 * slot + 1], s);
-  }
-};
+namespace mgpu {
 
 template <class T>
 inline cudaError_t launch_advance(const AdvanceArgs &A)
@@ -43,16 +28,22 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
   const T *F = (const T *) b.F[0], *G = (const T *) b.F[1], *H = (const T *) b.F[2];
 
   const unsigned zb = 256, fb = 128;
-  // learned guess on the tensor cores: persistent c2p kernel, at most 3 CTAs per SM
+  // learned guess on the tensor cores: persistent c2p kernel, MGPU_TC_CTAS_PER_SM CTAs per SM
+  // (4 x 128 threads x 128 registers fill the register file)
   const bool tc_c2p = A.pp.learned && A.pp.mlp_tc;
+  const bool simt_net = A.pp.learned && A.pp.mlp && !A.pp.mlp_tc;   // per-thread network guess
   const long long ntiles = (g.ninterior + 127) / 128;
-  const unsigned tcgrid = (unsigned) (ntiles < 148 * 3 ? ntiles : 148 * 3);
+  const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
+  const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
   auto c2p = [&](StateCPtr<T> Uin, int s, int zero_guess, int final) {
     if (tc_c2p)
       k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
                                                                 final, A.ereset, A.preset, A.dreset);
+    else if (simt_net)
+      k_cons_to_prim<T, 0><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
+          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
     else
-      k_cons_to_prim<T><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
+      k_cons_to_prim<T, 2><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
           g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
   };
   const unsigned zgrid = (unsigned) ((g.ninterior + zb - 1) / zb);

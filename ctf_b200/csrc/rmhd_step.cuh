@@ -19,6 +19,10 @@
 #ifndef MGPU_FLUX_MINB
 #define MGPU_FLUX_MINB 2
 #endif
+// The same for the zone c2p kernel (its natural register count allows 3 blocks).
+#ifndef MGPU_C2P_MINB
+#define MGPU_C2P_MINB 3
+#endif
 
 namespace mgpu {
 
@@ -166,8 +170,10 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
       }
 }
 
-// One interior zone's c2p (per-thread path, optional per-thread network guess).
-template <class T>
+// One interior zone's c2p.  Guess: 0 compiles in the per-thread network guess (used when
+// pp.learned), 2 leaves it out -- the network's activations would otherwise set the register
+// and stack budget of every c2p launch.
+template <class T, int Guess = 2>
 __device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, StatePtr<T> Pn, const PhysParams &pp,
                                          Ctl *ctl, int stage, int zero_guess, int final, int ereset, double preset,
                                          double dreset, long long t)
@@ -180,19 +186,19 @@ __device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, S
 #pragma unroll
   for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
   C2PTally tally;
-  const int err = cons_to_prim<(sizeof(T) < sizeof(double))>(pp, u, p, &tally) != 0;
+  const int err = cons_to_prim<(sizeof(T) < sizeof(double)), Guess>(pp, u, p, &tally) != 0;
   c2p_finish<T>(g, PA, Pn, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err, tally);
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
+template <class T, int Guess>
+__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
                                                       PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
                                                       int ereset, double preset, double dreset)
 {
   if (stage_failed(ctl, stage)) return;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.ninterior) return;
-  c2p_zone<T>(g, U, PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, t);
+  c2p_zone<T, Guess>(g, U, PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, t);
 }
 
 // ---- flux sweep (MethodOfLinesSplit::intercell_flux_sweep, Mara/plm-split.cpp:43-73) ---------

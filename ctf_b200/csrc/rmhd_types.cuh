@@ -102,6 +102,26 @@ struct LaunchProfiler {
   int *count;         // host counter
 };
 
+// Records an event pair around the launches of its scope when a profiler is attached.
+struct ProfScope {
+  LaunchProfiler *p;
+  cudaStream_t s;
+  int slot;
+  ProfScope(LaunchProfiler *p_, cudaStream_t s_, int tag, long long units) : p(p_), s(s_), slot(-1)
+  {
+    if (p && *p->count < p->capacity) {
+      slot = (*p->count)++;
+      p->tag[slot] = tag;
+      p->units[slot] = units;
+      cudaEventRecord(p->ev[2 * slot], s);
+    }
+  }
+  ~ProfScope()
+  {
+    if (slot >= 0) cudaEventRecord(p->ev[2 * slot + 1], s);
+  }
+};
+
 struct AdvanceArgs {
   Grid g;
   PhysParams pp;
@@ -149,6 +169,34 @@ struct TransferArgs {
   cudaStream_t stream;
 };
 
+// One member of an ensemble of boxes (device-side descriptor).
+struct BoxDev {
+  Grid g;
+  AdvanceBuffers b;
+  Ctl *ctl;
+  double min_dx;
+};
+
+// Launch arguments of an ensemble advance.
+struct EnsembleArgs {
+  const BoxDev *boxes;
+  int nb, nd;
+  const long long *zone_prefix;      // tiles of interior zones
+  const long long *face_prefix[3];   // tiles of faces per sweep direction
+  int zone_tile, face_tile;
+  int grid_zone, grid_face, grid_c2p;
+  long long total_zones, total_faces[3];   // work units, for the profiler
+  PhysParams pp;
+  int rk, ereset;
+  double preset, dreset;
+  int dt_mode;
+  const double *dt;   // per box (device), dt_mode 0
+  double cfl;
+  int commit;         // 0: leave every box's committed state as it was (launch-shape timing)
+  cudaStream_t stream;
+  LaunchProfiler *prof;   // nullptr: no timing (never set while capturing a graph)
+};
+
 }  // namespace mgpu
 
 // Entry points exported by each precision's translation unit.
@@ -158,5 +206,6 @@ struct TransferArgs {
   cudaError_t upload_##suffix(const TransferArgs &A, const double *d_aos, long long z0, long long count); \
   cudaError_t download_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count);     \
   cudaError_t face_io_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count, int to_aos); \
+  cudaError_t ensemble_advance_##suffix(const EnsembleArgs &E);                                          \
   }
 

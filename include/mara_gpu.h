@@ -173,6 +173,60 @@ int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, const double 
                          const void *dev_prim_in, void *dev_prim_out, double dt, int *errors,
                          double *max_lambda, void *stream, char *errbuf, int errbuf_len);
 
+/* ---- ensembles of independent boxes (no counterpart in the reference, whose solver is a
+ * process-global singleton, Mara/mara.cpp:135).  Every box of an ensemble has the same
+ * scheme (one mgpu_config) and dimensionality but its own size, extent, primitives, dt,
+ * MaxLambda, error counts and commit; box b advances exactly as an mgpu_solver of that box
+ * would.  One advance of the whole ensemble is a fixed sequence of persistent launches,
+ * each walking the tiles of all boxes, replayed as one CUDA graph.  Ng is 3; learned_c2p
+ * is not offered here. */
+typedef struct mgpu_ensemble mgpu_ensemble;
+
+/* Launch shape: tile lengths (contiguous flattened zones or faces per tile, multiples of
+ * 32) and persistent grid sizes (CTAs per SM) of the zone, face and c2p launches. */
+typedef struct {
+  int zone_tile, face_tile;
+  int zone_ctas_per_sm, face_ctas_per_sm, c2p_ctas_per_sm;
+} mgpu_ensemble_launch;
+
+/* N, x0, x1: nboxes * nd entries, box-major (x0/x1 NULL: the unit box for all). */
+int mgpu_ensemble_create(const mgpu_config *cfg, int nd, int nboxes, const int *N, const double *x0,
+                         const double *x1, mgpu_ensemble **out);
+int mgpu_ensemble_destroy(mgpu_ensemble *e);
+const char *mgpu_ensemble_last_error(const mgpu_ensemble *e);
+int mgpu_ensemble_set_stream(mgpu_ensemble *e, void *stream);
+int mgpu_ensemble_num_zones(const mgpu_ensemble *e, int box, long long *nz);   /* guarded zones */
+int mgpu_ensemble_total_interior(const mgpu_ensemble *e, long long *n);       /* over all boxes */
+int mgpu_ensemble_upload_prim(mgpu_ensemble *e, int box, const double *host_aos);
+int mgpu_ensemble_download_prim(mgpu_ensemble *e, int box, double *host_aos);
+int mgpu_ensemble_upload_prim_device(mgpu_ensemble *e, int box, const void *dev_aos);
+int mgpu_ensemble_download_prim_device(mgpu_ensemble *e, int box, void *dev_aos);
+int mgpu_ensemble_get_launch(const mgpu_ensemble *e, mgpu_ensemble_launch *L);
+int mgpu_ensemble_set_launch(mgpu_ensemble *e, const mgpu_ensemble_launch *L);
+/* Enqueue nsteps advances of every box.  dt_mode 0: box b uses dt[b] (host array, copied
+ * before the call returns); dt_mode 1: cfl * min_dx_b / MaxLambda_b of its previous advance.
+ * use_graph 1 replays a cached CUDA graph of the nsteps advances (captured on first use of
+ * a given nsteps, dt_mode, cfl and launch shape); 0 launches directly.  Asynchronous. */
+int mgpu_ensemble_advance(mgpu_ensemble *e, int nsteps, int dt_mode, const double *dt, double cfl,
+                          int use_graph);
+int mgpu_ensemble_synchronize(mgpu_ensemble *e);
+int mgpu_ensemble_errors(mgpu_ensemble *e, int *errors);          /* nboxes entries, last advance */
+int mgpu_ensemble_get_stats(mgpu_ensemble *e, int box, mgpu_stats *s);
+int mgpu_ensemble_get_timesteps(mgpu_ensemble *e, double cfl, double *dt);   /* nboxes entries */
+/* Per-kernel-class timing of direct (use_graph 0) advances, as mgpu_profile_*. */
+int mgpu_ensemble_profile_enable(mgpu_ensemble *e, int capacity);
+int mgpu_ensemble_profile_disable(mgpu_ensemble *e);
+int mgpu_ensemble_profile_read(mgpu_ensemble *e, double *ms, long long *launches, long long *units);
+/* Mean device time of one advance (dt_mode 0, dt[] per box) with launch shape L, over reps
+ * graph replays after one warm-up; nothing is committed and every box's state and control
+ * block are left as they were. */
+int mgpu_ensemble_time_advance(mgpu_ensemble *e, const mgpu_ensemble_launch *L, const double *dt, int reps,
+                               double *ms);
+/* Search the launch shapes (coordinate descent over tile lengths and grid sizes, timed with
+ * mgpu_ensemble_time_advance), install the fastest and return it and its time. */
+int mgpu_ensemble_autotune(mgpu_ensemble *e, const double *dt, int reps, mgpu_ensemble_launch *best,
+                           double *best_ms);
+
 #ifdef __cplusplus
 }
 #endif

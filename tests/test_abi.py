@@ -58,3 +58,32 @@ def test_null_handle_is_an_argument_error():
     lib = _lib.load()
     assert lib.mgpu_advance(None, 0.0, None) == 1
     assert lib.mgpu_destroy(None) == 0
+
+
+def test_ensemble_create_rejects_bad_arguments_without_a_gpu():
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    N = (ctypes.c_int * 4)(16, 16, 2, 16)
+    h = ctypes.c_void_p()
+    create = lib.mgpu_ensemble_create
+    assert create(ctypes.byref(c), 2, 2, N, None, None, ctypes.byref(h)) == 1     # N < 3 on an axis
+    assert create(ctypes.byref(c), 4, 1, N, None, None, ctypes.byref(h)) == 1     # 4 dimensions
+    assert create(ctypes.byref(c), 2, 0, N, None, None, ctypes.byref(h)) == 1     # no boxes
+    c.learned_c2p = 1
+    assert create(ctypes.byref(c), 2, 1, N, None, None, ctypes.byref(h)) == 5     # MGPU_ERR_UNSUPPORTED
+    assert not h.value
+    assert lib.mgpu_ensemble_advance(None, 1, 0, None, 0.0, 1) == 1
+    assert lib.mgpu_ensemble_destroy(None) == 1
+
+
+def test_ensemble_box_sizes_are_log_uniform():
+    import numpy as np
+    from ctf_b200.ensemble import kh_sizes
+    sizes = kh_sizes(256, seed=0)
+    sides = np.array([s[0] for s in sizes])
+    assert len(sizes) == 256 and all(s[0] == s[1] for s in sizes)
+    assert sides.min() >= 64 and sides.max() <= 512 and np.all(sides % 2 == 0)
+    # log-uniform: the median side is near the geometric mean sqrt(64 * 512) = 181
+    assert 150 <= np.median(sides) <= 215
+    assert kh_sizes(256, seed=0) == sizes

@@ -37,7 +37,9 @@ struct mgpu_ensemble {
   Ctl *ctl = nullptr;            // nb control blocks (device)
   Ctl *ctl_host = nullptr;       // pinned mirror
   BoxDev *boxes = nullptr;       // device descriptors
-  long long *prefix = nullptr;   // device: zone prefix (nb+1), then 3 face prefixes (nb+1 each)
+  int2 *maps = nullptr;          // device tile maps: zone tiles, then the face tiles of each sweep
+  size_t maps_cap = 0;           // entries allocated
+  size_t face_off[3] = {0, 0, 0};
   double *dt_dev = nullptr;      // per-box dt (device)
   double *staging = nullptr;     // AoS staging for host transfers
   long long staging_zones = 0;
@@ -129,24 +131,36 @@ Grid make_grid(int nd, const int *N, const double *x0, const double *x1, double 
 
 long long faces_of(const Grid &g, int dim) { return std::max(0ll, g.nz - 5 * g.s[dim - 1]); }
 
-// Tile prefixes for the current launch shape, uploaded to e->prefix.
-int build_prefixes(mgpu_ensemble *e)
+// Tile maps for the current launch shape: entry w of a map is (box, tile within the box) of
+// the w-th tile of the concatenated work; uploaded to e->maps.
+int build_maps(mgpu_ensemble *e)
 {
   const int nb = e->nb;
-  std::vector<long long> h(4 * (size_t) (nb + 1), 0);
   const long long zt = e->launch.zone_tile, ft = e->launch.face_tile;
+  std::vector<int2> h;
   for (int b = 0; b < nb; ++b) {
-    const Grid &g = e->grids[b];
-    h[b + 1] = h[b] + (g.ninterior + zt - 1) / zt;
-    for (int d = 0; d < 3; ++d) {
-      long long *p = h.data() + (size_t) (d + 1) * (nb + 1);
-      const long long nf = d < e->nd ? faces_of(g, d + 1) : 0;
-      p[b + 1] = p[b] + (nf + ft - 1) / ft;
-    }
+    const long long n = (e->grids[b].ninterior + zt - 1) / zt;
+    for (long long t = 0; t < n; ++t) h.push_back(make_int2(b, (int) t));
   }
-  e->zone_tiles = h[nb];
-  for (int d = 0; d < 3; ++d) e->face_tiles[d] = h[(size_t) (d + 1) * (nb + 1) + nb];
-  CK(cudaMemcpyAsync(e->prefix, h.data(), h.size() * sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+  e->zone_tiles = (long long) h.size();
+  for (int d = 0; d < 3; ++d) {
+    e->face_off[d] = h.size();
+    if (d < e->nd)
+      for (int b = 0; b < nb; ++b) {
+        const long long n = (faces_of(e->grids[b], d + 1) + ft - 1) / ft;
+        for (long long t = 0; t < n; ++t) h.push_back(make_int2(b, (int) t));
+      }
+    e->face_tiles[d] = (long long) (h.size() - e->face_off[d]);
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  if (h.size() > e->maps_cap) {
+    if (e->maps) cudaFree(e->maps);
+    e->maps = nullptr;
+    e->maps_cap = 0;
+    CK(cudaMalloc((void **) &e->maps, h.size() * sizeof(int2)));
+    e->maps_cap = h.size();
+  }
+  CK(cudaMemcpyAsync(e->maps, h.data(), h.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   return MGPU_OK;
 }
@@ -169,8 +183,12 @@ EnsembleArgs args_of(mgpu_ensemble *e, int dt_mode, double cfl, int commit, bool
   E.boxes = e->boxes;
   E.nb = nb;
   E.nd = e->nd;
-  E.zone_prefix = e->prefix;
-  for (int d = 0; d < 3; ++d) E.face_prefix[d] = e->prefix + (size_t) (d + 1) * (nb + 1);
+  E.zone_map = e->maps;
+  E.zone_tiles = e->zone_tiles;
+  for (int d = 0; d < 3; ++d) {
+    E.face_map[d] = e->maps + e->face_off[d];
+    E.face_tiles[d] = e->face_tiles[d];
+  }
   E.zone_tile = e->launch.zone_tile;
   E.face_tile = e->launch.face_tile;
   auto grid = [&](long long tiles, int cps) {
@@ -333,7 +351,7 @@ void release(mgpu_ensemble *e)
   if (e->arena) cudaFree(e->arena);
   if (e->ctl) cudaFree(e->ctl);
   if (e->boxes) cudaFree(e->boxes);
-  if (e->prefix) cudaFree(e->prefix);
+  if (e->maps) cudaFree(e->maps);
   if (e->dt_dev) cudaFree(e->dt_dev);
   if (e->staging) cudaFree(e->staging);
   if (e->ctl_host) cudaFreeHost(e->ctl_host);
@@ -406,7 +424,6 @@ int mgpu_ensemble_create(const mgpu_config *cfg, int nd, int nboxes, const int *
   if (c == cudaSuccess) c = cudaMemsetAsync(e->ctl, 0, sizeof(Ctl) * (size_t) nboxes, e->stream);
   if (c == cudaSuccess) c = cudaMallocHost((void **) &e->ctl_host, sizeof(Ctl) * (size_t) nboxes);
   if (c == cudaSuccess) c = cudaMalloc((void **) &e->boxes, sizeof(BoxDev) * (size_t) nboxes);
-  if (c == cudaSuccess) c = cudaMalloc((void **) &e->prefix, sizeof(long long) * 4 * (size_t) (nboxes + 1));
   if (c == cudaSuccess) c = cudaMalloc((void **) &e->dt_dev, sizeof(double) * (size_t) nboxes);
   if (c == cudaSuccess) c = cudaMemsetAsync(e->dt_dev, 0, sizeof(double) * (size_t) nboxes, e->stream);
   e->staging_zones = std::min<long long>(max_nz, 1ll << 22);
@@ -461,7 +478,7 @@ int mgpu_ensemble_create(const mgpu_config *cfg, int nd, int nboxes, const int *
   e->launch.zone_ctas_per_sm = 8;
   e->launch.face_ctas_per_sm = fp32(e) ? 4 : 3;
   e->launch.c2p_ctas_per_sm = 8;
-  if (build_prefixes(e)) {
+  if (build_maps(e)) {
     fprintf(stderr, "[mgpu] ensemble: %s\n", e->err.c_str());
     release(e);
     delete e;
@@ -548,7 +565,7 @@ int mgpu_ensemble_set_launch(mgpu_ensemble *e, const mgpu_ensemble_launch *L)
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   e->launch = *L;
-  return build_prefixes(e);
+  return build_maps(e);
 }
 
 int mgpu_ensemble_advance(mgpu_ensemble *e, int nsteps, int dt_mode, const double *dt, double cfl, int use_graph)
@@ -676,7 +693,7 @@ int mgpu_ensemble_time_advance(mgpu_ensemble *e, const mgpu_ensemble_launch *L, 
   if (rc) return rc;
   std::vector<Ctl> saved(e->ctl_host, e->ctl_host + e->nb);
   e->launch = *L;
-  rc = build_prefixes(e);
+  rc = build_maps(e);
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (!rc) {
     CK(cudaMemcpyAsync(e->dt_dev, dt, sizeof(double) * (size_t) e->nb, cudaMemcpyHostToDevice, e->stream));
@@ -695,7 +712,7 @@ int mgpu_ensemble_time_advance(mgpu_ensemble *e, const mgpu_ensemble_launch *L, 
   if (t1) cudaEventDestroy(t1);
   drop_graph(e);
   e->launch = keep;
-  const int rc2 = build_prefixes(e);
+  const int rc2 = build_maps(e);
   memcpy(e->ctl_host, saved.data(), sizeof(Ctl) * (size_t) e->nb);
   CK(cudaMemcpyAsync(e->ctl, e->ctl_host, sizeof(Ctl) * (size_t) e->nb, cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));

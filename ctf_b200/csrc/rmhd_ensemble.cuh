@@ -3,26 +3,28 @@
 //
 // Every phase of the step (P->U, c2p, the flux sweeps, the CT + divergence + RK update) is one
 // persistent launch over the concatenated work of all boxes: the work of box b is cut into
-// tiles (`tile` zones or faces), the tiles of all boxes are numbered consecutively
-// (prefix[b] = first tile of box b), and each CTA walks tiles w = blockIdx.x, +gridDim.x, ...
-// finding its box by binary search of the prefix array.  A tile never spans two boxes, so a
-// CTA's block-level reductions (MaxLambda) and its stage-failure early exit stay per box.
-// Each box keeps its own control block: its own dt, MaxLambda, error counts and commit.
-// The per-item work is the single-box kernels' device bodies (rmhd_step.cuh).
+// tiles (`tile` consecutive interior zones, or faces of a sweep), the tiles of all boxes are
+// numbered consecutively, and a map gives each tile its (box, tile-within-box).  Each CTA
+// walks tiles w = blockIdx.x, +gridDim.x, ...; per tile it reads its map entry and stages
+// the box's descriptor in shared memory (one coalesced copy), then runs the single-box
+// kernels' device bodies (rmhd_step.cuh) on the tile.  A tile never spans two boxes, so a
+// CTA's block-level reductions (MaxLambda) and its stage-failure early exit stay per box;
+// each box keeps its own control block: its own dt, MaxLambda, error counts and commit.
 #pragma once
 #include "rmhd_step.cuh"
 
 namespace mgpu {
 
-__device__ __forceinline__ int find_box(const long long *prefix, int nb, long long w)
+static_assert(sizeof(BoxDev) % 8 == 0, "BoxDev is copied in 8-byte words");
+
+// Stage box `src`'s descriptor in shared memory (all threads of the CTA call this).
+__device__ __forceinline__ void load_box(BoxDev &sd, const BoxDev *src)
 {
-  int lo = 0, hi = nb;   // invariant: prefix[lo] <= w < prefix[hi]
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (prefix[mid] <= w) lo = mid;
-    else hi = mid;
-  }
-  return lo;
+  __syncthreads();   // every thread is done with the previous tile's descriptor
+  constexpr int W = (int) (sizeof(BoxDev) / 8);
+  for (int i = threadIdx.x; i < W; i += blockDim.x)
+    reinterpret_cast<long long *>(&sd)[i] = reinterpret_cast<const long long *>(src)[i];
+  __syncthreads();
 }
 
 template <class T> __device__ __forceinline__ StatePtr<T> box_state(void *bulk, double *B) { return {(T *) bulk, B}; }
@@ -65,14 +67,14 @@ static __global__ void k_ens_commit(const BoxDev *boxes, int nb, int nstages, in
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_ens_p2c(const BoxDev *boxes, const long long *prefix, int nb, int tile,
+__global__ void __launch_bounds__(256) k_ens_p2c(const BoxDev *boxes, const int2 *map, long long ntiles, int tile,
                                                  double gamma)
 {
-  const long long total = prefix[nb];
-  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
-    const int bi = find_box(prefix, nb, w);
-    const BoxDev &d = boxes[bi];
-    const long long base = (w - prefix[bi]) * tile;
+  __shared__ BoxDev d;
+  for (long long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+    const int2 m = map[w];
+    load_box(d, boxes + m.x);
+    const long long base = (long long) m.y * tile;
     const int cur = d.ctl->cur;
     const StateCPtr<T> P = box_cstate<T>(d.b.Pc_bulk[cur], d.b.Pc_B[cur]);
     const StatePtr<T> U = box_state<T>(d.b.U0_bulk, d.b.U0_B);
@@ -85,16 +87,16 @@ __global__ void __launch_bounds__(256) k_ens_p2c(const BoxDev *boxes, const long
 
 // uin: 0 reads U0, 1 reads U1
 template <class T>
-__global__ void __launch_bounds__(128) k_ens_c2p(const BoxDev *boxes, const long long *prefix, int nb, int tile,
+__global__ void __launch_bounds__(128) k_ens_c2p(const BoxDev *boxes, const int2 *map, long long ntiles, int tile,
                                                  PhysParams pp, int stage, int uin, int zero_guess, int final,
                                                  int ereset, double preset, double dreset)
 {
-  const long long total = prefix[nb];
-  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
-    const int bi = find_box(prefix, nb, w);
-    const BoxDev &d = boxes[bi];
-    if (stage_failed(d.ctl, stage)) continue;
-    const long long base = (w - prefix[bi]) * tile;
+  __shared__ BoxDev d;
+  for (long long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+    const int2 m = map[w];
+    load_box(d, boxes + m.x);
+    if (stage_failed(d.ctl, stage)) continue;   // uniform over the block
+    const long long base = (long long) m.y * tile;
     const StateCPtr<T> U = uin ? box_cstate<T>(d.b.U1_bulk, d.b.U1_B) : box_cstate<T>(d.b.U0_bulk, d.b.U0_B);
     const int nxt = d.ctl->cur ^ 1;
     const StatePtr<T> Pn = box_state<T>(d.b.Pc_bulk[nxt], d.b.Pc_B[nxt]);
@@ -107,17 +109,18 @@ __global__ void __launch_bounds__(128) k_ens_c2p(const BoxDev *boxes, const long
 }
 
 template <class T, int dim>
-__global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *boxes, const long long *prefix,
-                                                                  int nb, int tile, PhysParams pp, int stage)
+__global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *boxes, const int2 *map,
+                                                                  long long ntiles, int tile, PhysParams pp,
+                                                                  int stage)
 {
-  const long long total = prefix[nb];
+  __shared__ BoxDev d;
   const bool hlld = pp.riemann == RIEMANN_HLLD;
-  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
-    const int bi = find_box(prefix, nb, w);
-    const BoxDev &d = boxes[bi];
-    if (stage_failed(d.ctl, stage + 1)) continue;   // uniform over the block: one box per tile
+  for (long long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+    const int2 m = map[w];
+    load_box(d, boxes + m.x);
+    if (stage_failed(d.ctl, stage + 1)) continue;   // uniform over the block
     const long long S = d.g.s[dim - 1];
-    const long long base = 2 * S + (w - prefix[bi]) * tile;
+    const long long base = 2 * S + (long long) m.y * tile;
     const long long end = d.g.nz - 3 * S;
     T ml = T(0);
     FluxTally ft{0, 0, 0, 0, 0};
@@ -129,17 +132,22 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *
   }
 }
 
-// out: 0 writes U0, 1 writes U1; kout: -1 none, else K[kout] (RK4)
-template <class T>
-__global__ void __launch_bounds__(256) k_ens_update(const BoxDev *boxes, const long long *prefix, int nb, int tile,
-                                                    UpdateArgs a, int stage, int out, int kout)
+// out: 0 writes U0, 1 writes U1; kout: -1 none, else K[kout] (RK4).  ND: the boxes' common
+// dimensionality.  At least MGPU_ENS_UPDATE_MINB resident blocks (an HBM-bound kernel wants
+// occupancy more than the loop-invariant box fields the compiler would otherwise hoist).
+#ifndef MGPU_ENS_UPDATE_MINB
+#define MGPU_ENS_UPDATE_MINB 3
+#endif
+template <class T, int ND>
+__global__ void __launch_bounds__(256, MGPU_ENS_UPDATE_MINB) k_ens_update(const BoxDev *boxes, const int2 *map, long long ntiles,
+                                                    int tile, UpdateArgs a, int stage, int out, int kout)
 {
-  const long long total = prefix[nb];
-  for (long long w = blockIdx.x; w < total; w += gridDim.x) {
-    const int bi = find_box(prefix, nb, w);
-    const BoxDev &d = boxes[bi];
+  __shared__ BoxDev d;
+  for (long long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+    const int2 m = map[w];
+    load_box(d, boxes + m.x);
     if (stage_failed(d.ctl, stage + 1)) continue;
-    const long long base = (w - prefix[bi]) * tile;
+    const long long base = (long long) m.y * tile;
     const StateCPtr<T> U0 = box_cstate<T>(d.b.U0_bulk, d.b.U0_B), U1 = box_cstate<T>(d.b.U1_bulk, d.b.U1_B);
     const StatePtr<T> Uout = out ? box_state<T>(d.b.U1_bulk, d.b.U1_B) : box_state<T>(d.b.U0_bulk, d.b.U0_B);
     StatePtr<T> Kout{nullptr, nullptr};
@@ -150,7 +158,7 @@ __global__ void __launch_bounds__(256) k_ens_update(const BoxDev *boxes, const l
     for (int s = threadIdx.x; s < tile; s += blockDim.x) {
       const long long t = base + s;
       if (t < d.g.ninterior)
-        update_zone<T>(d.g, a, U0, U1, (const T *) d.b.F[0], (const T *) d.b.F[1], (const T *) d.b.F[2], Uout,
+        update_zone<T, ND>(d.g, a, U0, U1, (const T *) d.b.F[0], (const T *) d.b.F[1], (const T *) d.b.F[2], Uout,
                        Kout, K1, K2, K3, dt, t);
     }
   }
@@ -168,23 +176,26 @@ inline cudaError_t launch_ensemble_advance(const EnsembleArgs &E)
   }
   {
     ProfScope ps(pr, st, KC_P2C, E.total_zones);
-    k_ens_p2c<T><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_prefix, nb, E.zone_tile, E.pp.gamma);
+    k_ens_p2c<T><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, E.pp.gamma);
   }
   const int ns = num_stages(E.rk);
   for (int s = 0; s < ns; ++s) {
     {
       ProfScope ps(pr, st, KC_C2P, E.total_zones);
-      k_ens_c2p<T><<<E.grid_c2p, 128, 0, st>>>(E.boxes, E.zone_prefix, nb, E.zone_tile, E.pp, s, s == 0 ? 0 : 1,
+      k_ens_c2p<T><<<E.grid_c2p, 128, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, E.pp, s, s == 0 ? 0 : 1,
                                                s == 0, 0, E.ereset, E.preset, E.dreset);
     }
     for (int d = 1; d <= E.nd; ++d) {
       ProfScope ps(pr, st, KC_FLUX, E.total_faces[d - 1]);
       if (d == 1)
-        k_ens_flux<T, 1><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_prefix[0], nb, E.face_tile, E.pp, s);
+        k_ens_flux<T, 1><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[0], E.face_tiles[0],
+                                                      E.face_tile, E.pp, s);
       else if (d == 2)
-        k_ens_flux<T, 2><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_prefix[1], nb, E.face_tile, E.pp, s);
+        k_ens_flux<T, 2><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[1], E.face_tiles[1],
+                                                      E.face_tile, E.pp, s);
       else
-        k_ens_flux<T, 3><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_prefix[2], nb, E.face_tile, E.pp, s);
+        k_ens_flux<T, 3><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[2], E.face_tiles[2],
+                                                      E.face_tile, E.pp, s);
     }
     const StageKind kind = stage_kind(E.rk, s);
     const UpdateArgs ua{kind.combine, kind.c};
@@ -198,11 +209,16 @@ inline cudaError_t launch_ensemble_advance(const EnsembleArgs &E)
       out = (s == ns - 1) ? 0 : 1;
     }
     ProfScope ps(pr, st, KC_UPDATE, E.total_zones);
-    k_ens_update<T><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_prefix, nb, E.zone_tile, ua, s, out, kout);
+    if (E.nd == 1)
+      k_ens_update<T, 1><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, ua, s, out, kout);
+    else if (E.nd == 2)
+      k_ens_update<T, 2><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, ua, s, out, kout);
+    else
+      k_ens_update<T, 3><<<E.grid_zone, 256, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, ua, s, out, kout);
   }
   {
     ProfScope ps(pr, st, KC_C2P, E.total_zones);
-    k_ens_c2p<T><<<E.grid_c2p, 128, 0, st>>>(E.boxes, E.zone_prefix, nb, E.zone_tile, E.pp, ns, 0, 0, 1, E.ereset,
+    k_ens_c2p<T><<<E.grid_c2p, 128, 0, st>>>(E.boxes, E.zone_map, E.zone_tiles, E.zone_tile, E.pp, ns, 0, 0, 1, E.ereset,
                                              E.preset, E.dreset);
   }
   {

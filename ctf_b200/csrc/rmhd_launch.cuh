@@ -87,9 +87,14 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
       Uout = (s == ns - 1) ? U0 : U1;
     }
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
-    k_update<T><<<zgrid, zb, 0, st>>>(g, ua, StateCPtr<T>{U0.bulk, U0.B}, StateCPtr<T>{U1.bulk, U1.B}, F, G, H, Uout,
-                                      Kout, StateCPtr<T>{K[0].bulk, K[0].B}, StateCPtr<T>{K[1].bulk, K[1].B},
-                                      StateCPtr<T>{K[2].bulk, K[2].B}, A.ctl, s);
+    const StateCPtr<T> cU0{U0.bulk, U0.B}, cU1{U1.bulk, U1.B}, cK0{K[0].bulk, K[0].B}, cK1{K[1].bulk, K[1].B},
+        cK2{K[2].bulk, K[2].B};
+    if (g.nd == 1)
+      k_update<T, 1><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
+    else if (g.nd == 2)
+      k_update<T, 2><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
+    else
+      k_update<T, 3><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
   }
   {
     ProfScope ps(pr, st, KC_C2P, g.ninterior);

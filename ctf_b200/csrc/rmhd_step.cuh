@@ -354,7 +354,7 @@ __device__ __forceinline__ T combine_bulk(const UpdateArgs &a, T un, T us, T dt,
   }
 }
 
-template <class T>
+template <class T, int ND>
 __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, StateCPtr<T> Un, StateCPtr<T> Us,
                                             const T *__restrict__ F, const T *__restrict__ G,
                                             const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
@@ -372,9 +372,9 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
     T L;
-    if (g.nd == 1) {
+    if (ND == 1) {
       L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx);
-    } else if (g.nd == 2) {
+    } else if (ND == 2) {
       L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx) - (G[q * g.cs + z] - G[q * g.cs + z - sy]) / T(dy);
     } else {
       L = -(F[q * g.cs + z] - F[q * g.cs + z - sx]) / T(dx) - (G[q * g.cs + z] - G[q * g.cs + z - sy]) / T(dy) -
@@ -389,10 +389,10 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
   }
   // magnetic components 5..7 in double, with the constrained-transport fluxes
   double Lb[3];
-  if (g.nd == 1) {
+  if (ND == 1) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) Lb[c] = -(fval(F, g, 5 + c, z) - fval(F, g, 5 + c, z - sx)) / dx;
-  } else if (g.nd == 2) {
+  } else if (ND == 2) {
     // CT2d: Fx[Bx] = 0, Fx[By] = FxBy, Fy[Bx] = FyBx, Fy[By] = 0; Bz keeps its Godunov fluxes
     const double FxBy0 = ct_emf(F, G, g, By, Bx, z, sx, sy), FxBym = ct_emf(F, G, g, By, Bx, z - sx, sx, sy);
     const double FyBx0 = ct_emf(G, F, g, Bx, By, z, sy, sx), FyBxm = ct_emf(G, F, g, Bx, By, z - sy, sy, sx);
@@ -429,7 +429,7 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
   }
 }
 
-template <class T>
+template <class T, int ND>
 __global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
                                                 const T *__restrict__ F, const T *__restrict__ G,
                                                 const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<
   if (stage_failed(ctl, stage + 1)) return;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.ninterior) return;
-  update_zone<T>(g, a, Un, Us, F, G, H, Uout, Kout, K1, K2, K3, ctl->dt, t);
+  update_zone<T, ND>(g, a, Un, Us, F, G, H, Uout, Kout, K1, K2, K3, ctl->dt, t);
 }
 
 }  // namespace mgpu

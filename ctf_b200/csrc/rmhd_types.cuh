@@ -181,8 +181,9 @@ struct BoxDev {
 struct EnsembleArgs {
   const BoxDev *boxes;
   int nb, nd;
-  const long long *zone_prefix;      // tiles of interior zones
-  const long long *face_prefix[3];   // tiles of faces per sweep direction
+  const int2 *zone_map;              // per tile of interior zones: (box, tile within the box)
+  const int2 *face_map[3];           // the same for the faces of each sweep direction
+  long long zone_tiles, face_tiles[3];
   int zone_tile, face_tile;
   int grid_zone, grid_face, grid_c2p;
   long long total_zones, total_faces[3];   // work units, for the profiler

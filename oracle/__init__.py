@@ -238,6 +238,20 @@ class RefOracle:
         if self.lib.ref_dostring(code.encode()):
             raise RuntimeError(self.lib.ref_last_error().decode())
 
+    def dostring(self, code: str, quiet: bool = True):
+        """Run Lua code in the reference's interpreter (`Mara` and `buffer` preloaded)."""
+        if not quiet:
+            return self._do(code)
+        fd = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        try:
+            self._do(code)
+        finally:
+            os.dup2(fd, 1)
+            os.close(fd)
+            os.close(devnull)
+
     def close(self):
         self.lib.ref_close()
 

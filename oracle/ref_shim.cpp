@@ -21,6 +21,7 @@ extern "C" {
 #include "weno.h"
 #include "rmhd-c2p.h"
 int luaopen_Mara(lua_State *L);
+int luaopen_buffer(lua_State *L);
 }
 #include "hydro.hpp"
 #include "rmhd.hpp"
@@ -44,6 +45,8 @@ int ref_open(void)
   L = luaL_newstate();
   luaL_openlibs(L);
   luaL_requiref(L, "Mara", luaopen_Mara, 1);
+  lua_pop(L, 1);
+  luaL_requiref(L, "buffer", luaopen_buffer, 1);   /* as ctf-core/ctf.c preloads it */
   lua_pop(L, 1);
   return 0;
 }

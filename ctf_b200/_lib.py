@@ -92,6 +92,13 @@ SIGNATURES = {
     "mgpu_mlp_build_tc_image": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _vp]),
     "mgpu_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), _dp, _dp, _ip, ctypes.c_int, _vp, _vp,
                                             ctypes.c_double, _ip, _dp, _vp, ctypes.c_char_p, ctypes.c_int]),
+    "mgpu_advance_phase": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double]),
+    "mgpu_reduction_targets": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "mgpu_set_external_guards": (ctypes.c_int, [_vp, _ip, _ip]),
+    "mgpu_halo_bytes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_halo_pack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "mgpu_halo_unpack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "mgpu_ensemble_create": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), ctypes.c_int, ctypes.c_int, _ip, _dp, _dp,
                                             ctypes.POINTER(_vp)]),
     "mgpu_ensemble_destroy": (ctypes.c_int, [_vp]),

@@ -287,6 +287,7 @@ TransferArgs transfer_args(const mgpu_ensemble *e, int box)
   t.b = e->bufs[box];
   t.ctl = e->ctl + box;
   t.stream = e->stream;
+  t.cur = 0;
   return t;
 }
 

@@ -39,6 +39,7 @@ struct mgpu_solver {
   float *mlp = nullptr;         // learned c2p network (device)
   long long mlp_count = 0;
   void *mlp_tc = nullptr;       // its tensor-core image (device)
+  int *mult = nullptr;          // multiplicity tables of a decomposed domain (device)
   // kernel timing
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_tag;
@@ -114,6 +115,7 @@ TransferArgs transfer_args(mgpu_solver *h)
   t.b = h->b;
   t.ctl = h->ctl;
   t.stream = h->stream;
+  t.cur = 0;
   return t;
 }
 
@@ -302,6 +304,7 @@ int mgpu_destroy(mgpu_solver *h)
   prof_free(h);
   if (h->mlp) cudaFree(h->mlp);
   if (h->mlp_tc) cudaFree(h->mlp_tc);
+  if (h->mult) cudaFree(h->mult);
   if (h->ctl) cudaFree(h->ctl);
   if (h->ctl_host) cudaFreeHost(h->ctl_host);
   if (h->red_host) cudaFreeHost(h->red_host);
@@ -337,6 +340,8 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
     if (N[d] < ng) return fail(h, MGPU_ERR_ARG, "periodic guard fill needs N >= Ng on every axis");
   CK(cudaStreamSynchronize(h->stream));
   free_buffers(h);
+  if (h->mult) cudaFree(h->mult);
+  h->mult = nullptr;
   h->have_domain = false;
   Grid &g = h->g;
   g = Grid{};
@@ -711,6 +716,114 @@ int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long
   }
   h->prof_count = 0;
   return MGPU_OK;
+}
+
+int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double dt, double cfl)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  const int ns = num_stages(h->cfg.rk);
+  if (phase < 0 || phase > 3 || stage < 0 || stage > ns || (phase == 2 && stage >= ns) ||
+      (dt_mode != 0 && dt_mode != 1))
+    return fail(h, MGPU_ERR_ARG, "bad advance phase arguments");
+  AdvanceArgs A;
+  A.g = h->g;
+  A.pp = phys(h);
+  A.rk = h->cfg.rk;
+  A.ereset = h->cfg.ereset;
+  A.preset = h->cfg.preset;
+  A.dreset = h->cfg.dreset;
+  A.dt_mode = dt_mode;
+  A.dt = dt;
+  A.cfl = cfl;
+  A.min_dx = h->min_dx;
+  A.b = h->b;
+  A.ctl = h->ctl;
+  A.stream = h->stream;
+  A.prof = h->prof_on ? &h->prof : nullptr;
+  CK(fp32(h) ? phase_fp32(A, phase, stage) : phase_fp64(A, phase, stage));
+  return MGPU_OK;
+}
+
+int mgpu_reduction_targets(mgpu_solver *h, void **err_counts, void **max_lambda_bits)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (err_counts) *err_counts = (void *) &h->ctl->stage_err[0];
+  if (max_lambda_bits) *max_lambda_bits = (void *) &h->ctl->max_lambda_bits;
+  return MGPU_OK;
+}
+
+int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (!ext) return fail(h, MGPU_ERR_ARG, "null ext");
+  CK(cudaStreamSynchronize(h->stream));
+  Grid &g = h->g;
+  long long total = 0;
+  for (int d = 0; d < g.nd; ++d)
+    if (ext[d]) total += g.n[d];
+  if (total > 0 && !mult) return fail(h, MGPU_ERR_ARG, "external guards need multiplicity tables");
+  for (long long i = 0; i < total; ++i)
+    if (mult[i] < 1) return fail(h, MGPU_ERR_ARG, "multiplicities must be >= 1");
+  if (h->mult) cudaFree(h->mult);
+  h->mult = nullptr;
+  for (int d = 0; d < 3; ++d) {
+    g.ext[d] = 0;
+    g.mult[d] = nullptr;
+  }
+  if (total == 0) return MGPU_OK;
+  CK(cudaMalloc((void **) &h->mult, sizeof(int) * (size_t) total));
+  CK(cudaMemcpy(h->mult, mult, sizeof(int) * (size_t) total, cudaMemcpyHostToDevice));
+  long long off = 0;
+  for (int d = 0; d < g.nd; ++d)
+    if (ext[d]) {
+      g.ext[d] = 1;
+      g.mult[d] = h->mult + off;
+      off += g.n[d];
+    }
+  return MGPU_OK;
+}
+
+int mgpu_halo_bytes(mgpu_solver *h, int which, int dim, long long *bytes)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (!bytes || dim < 0 || dim >= h->g.nd || (which != 0 && which != 1)) return fail(h, MGPU_ERR_ARG, "bad halo arguments");
+  const Grid &g = h->g;
+  const long long cross = dim == 0 ? (long long) g.G[1] * g.G[2] : dim == 1 ? (long long) g.G[0] * g.G[2]
+                                                                          : (long long) g.G[0] * g.G[1];
+  const long long per = cross * g.ng;
+  const long long tsz = fp32(h) ? 4 : 8;
+  *bytes = which == 0 ? per * 8 * tsz : per * (5 * tsz + 3 * 8);
+  return MGPU_OK;
+}
+
+static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pack)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (!buf || dim < 0 || dim >= h->g.nd || (which != 0 && which != 1) || (side != 0 && side != 1))
+    return fail(h, MGPU_ERR_ARG, "bad halo arguments");
+  TransferArgs t = transfer_args(h);
+  if (which == 1) {
+    rc = read_ctl(h);
+    if (rc) return rc;
+    t.cur = h->ctl_host->cur;
+  }
+  CK(fp32(h) ? halo_fp32(t, which, dim, side, buf, pack) : halo_fp64(t, which, dim, side, buf, pack));
+  return MGPU_OK;
+}
+
+int mgpu_halo_pack(mgpu_solver *h, int which, int dim, int side, void *dev_buf)
+{
+  return halo(h, which, dim, side, dev_buf, 1);
+}
+
+int mgpu_halo_unpack(mgpu_solver *h, int which, int dim, int side, const void *dev_buf)
+{
+  return halo(h, which, dim, side, const_cast<void *>(dev_buf), 0);
 }
 
 // Grid, buffers and stream of a solver, for the learned-c2p harvest (c2p_mlp.cu).

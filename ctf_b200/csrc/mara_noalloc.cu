@@ -168,6 +168,7 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   t.b = b;
   t.ctl = ctl;
   t.stream = st;
+  t.cur = 0;
   if (e == cudaSuccess) e = upload_fp64(t, (const double *) dev_prim_in, 0, g.nz);
 
   AdvanceArgs A;

@@ -108,13 +108,13 @@ __global__ void __launch_bounds__(128) k_ens_c2p(const BoxDev *boxes, const int2
   }
 }
 
-template <class T, int dim>
+template <class T, int dim, int RS>
 __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *boxes, const int2 *map,
                                                                   long long ntiles, int tile, PhysParams pp,
                                                                   int stage)
 {
   __shared__ BoxDev d;
-  const bool hlld = pp.riemann == RIEMANN_HLLD;
+  constexpr bool hlld = RS == RIEMANN_HLLD;
   for (long long w = blockIdx.x; w < ntiles; w += gridDim.x) {
     const int2 m = map[w];
     load_box(d, boxes + m.x);
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *
     FluxTally ft{0, 0, 0, 0, 0};
     for (int s = threadIdx.x; s < tile; s += blockDim.x) {
       const long long f = base + s;
-      if (f < end) flux_face<T, dim>(d.g, (const T *) d.b.PA, (T *) d.b.F[dim - 1], pp, f, ml, ft);
+      if (f < end) flux_face<T, dim, RS>(d.g, (const T *) d.b.PA, (T *) d.b.F[dim - 1], pp, f, ml, ft);
     }
     flux_block_finish(double(ml), ft, d.ctl, hlld);
   }
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_ens_flux(const BoxDev *
 // dimensionality.  At least MGPU_ENS_UPDATE_MINB resident blocks (an HBM-bound kernel wants
 // occupancy more than the loop-invariant box fields the compiler would otherwise hoist).
 #ifndef MGPU_ENS_UPDATE_MINB
-#define MGPU_ENS_UPDATE_MINB 3
+#define MGPU_ENS_UPDATE_MINB 4   // chosen by a sweep of 2-4
 #endif
 template <class T, int ND>
 __global__ void __launch_bounds__(256, MGPU_ENS_UPDATE_MINB) k_ens_update(const BoxDev *boxes, const int2 *map, long long ntiles,
@@ -165,6 +165,21 @@ __global__ void __launch_bounds__(256, MGPU_ENS_UPDATE_MINB) k_ens_update(const 
 }
 
 template <class T>
+inline void launch_ens_flux(const EnsembleArgs &E, int d, int s)
+{
+#define MGPU_ENS_FLUX_CASE(D, R)                                                                             \
+  if (d == D && E.pp.riemann == R) {                                                                         \
+    k_ens_flux<T, D, R><<<E.grid_face, 128, 0, E.stream>>>(E.boxes, E.face_map[D - 1], E.face_tiles[D - 1], \
+                                                           E.face_tile, E.pp, s);                            \
+    return;                                                                                                  \
+  }
+  MGPU_ENS_FLUX_CASE(1, RIEMANN_HLLD) MGPU_ENS_FLUX_CASE(2, RIEMANN_HLLD) MGPU_ENS_FLUX_CASE(3, RIEMANN_HLLD)
+  MGPU_ENS_FLUX_CASE(1, RIEMANN_HLLC) MGPU_ENS_FLUX_CASE(2, RIEMANN_HLLC) MGPU_ENS_FLUX_CASE(3, RIEMANN_HLLC)
+  MGPU_ENS_FLUX_CASE(1, RIEMANN_HLL) MGPU_ENS_FLUX_CASE(2, RIEMANN_HLL) MGPU_ENS_FLUX_CASE(3, RIEMANN_HLL)
+#undef MGPU_ENS_FLUX_CASE
+}
+
+template <class T>
 inline cudaError_t launch_ensemble_advance(const EnsembleArgs &E)
 {
   cudaStream_t st = E.stream;
@@ -187,15 +202,7 @@ inline cudaError_t launch_ensemble_advance(const EnsembleArgs &E)
     }
     for (int d = 1; d <= E.nd; ++d) {
       ProfScope ps(pr, st, KC_FLUX, E.total_faces[d - 1]);
-      if (d == 1)
-        k_ens_flux<T, 1><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[0], E.face_tiles[0],
-                                                      E.face_tile, E.pp, s);
-      else if (d == 2)
-        k_ens_flux<T, 2><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[1], E.face_tiles[1],
-                                                      E.face_tile, E.pp, s);
-      else
-        k_ens_flux<T, 3><<<E.grid_face, 128, 0, st>>>(E.boxes, E.face_map[2], E.face_tiles[2],
-                                                      E.face_tile, E.pp, s);
+      launch_ens_flux<T>(E, d, s);
     }
     const StageKind kind = stage_kind(E.rk, s);
     const UpdateArgs ua{kind.combine, kind.c};

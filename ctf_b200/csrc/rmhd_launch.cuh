@@ -3,6 +3,7 @@
 //   -> closing c2p into the uncommitted prim buffer -> commit if no zone failed.
 // Nothing is read back: the host learns the outcome from the control block when it asks.
 #pragma once
+#include <algorithm>
 #include "rmhd_step.cuh"
 #include "rmhd_step_tc.cuh"
 
@@ -12,8 +13,31 @@
 
 namespace mgpu {
 
+// One sweep: the flux kernel for (sweep direction, Riemann solver), both compile-time.
 template <class T>
-inline cudaError_t launch_advance(const AdvanceArgs &A)
+inline void launch_flux(const Grid &g, int d, int rs, unsigned grid, unsigned blk, cudaStream_t st, const T *PA,
+                        T *F, const PhysParams &pp, Ctl *ctl, int s)
+{
+#define MGPU_FLUX_CASE(D, R)                                                            \
+  if (d == D && rs == R) {                                                              \
+    k_flux<T, D, R><<<grid, blk, 0, st>>>(g, PA, F, pp, ctl, s);                        \
+    return;                                                                             \
+  }
+  MGPU_FLUX_CASE(1, RIEMANN_HLLD) MGPU_FLUX_CASE(2, RIEMANN_HLLD) MGPU_FLUX_CASE(3, RIEMANN_HLLD)
+  MGPU_FLUX_CASE(1, RIEMANN_HLLC) MGPU_FLUX_CASE(2, RIEMANN_HLLC) MGPU_FLUX_CASE(3, RIEMANN_HLLC)
+  MGPU_FLUX_CASE(1, RIEMANN_HLL) MGPU_FLUX_CASE(2, RIEMANN_HLL) MGPU_FLUX_CASE(3, RIEMANN_HLL)
+#undef MGPU_FLUX_CASE
+}
+
+// Phases of an advance.  The whole advance is PH_BEGIN, then (PH_C2P, PH_FLUX_UPDATE) per RK
+// stage, then PH_C2P with stage = number of stages (the closing c2p into the uncommitted
+// buffer), then PH_COMMIT.  A decomposed domain exchanges the guard layers of the stage
+// primitives between PH_C2P and PH_FLUX_UPDATE, and sums the error counters over ranks
+// before PH_COMMIT.
+enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3 };
+
+template <class T>
+inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
 {
   const Grid &g = A.g;
   const AdvanceBuffers &b = A.b;
@@ -26,16 +50,34 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
   for (int i = 0; i < 3; ++i) K[i] = state(b.K_bulk[i], b.K_B[i]);
   T *PA = (T *) b.PA;
   const T *F = (const T *) b.F[0], *G = (const T *) b.F[1], *H = (const T *) b.F[2];
+  const int ns = num_stages(A.rk);
 
   const unsigned zb = 256, fb = 128;
-  // learned guess on the tensor cores: persistent c2p kernel, MGPU_TC_CTAS_PER_SM CTAs per SM
-  // (4 x 128 threads x 128 registers fill the register file)
-  const bool tc_c2p = A.pp.learned && A.pp.mlp_tc;
-  const bool simt_net = A.pp.learned && A.pp.mlp && !A.pp.mlp_tc;   // per-thread network guess
-  const long long ntiles = (g.ninterior + 127) / 128;
-  const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
-  const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
-  auto c2p = [&](StateCPtr<T> Uin, int s, int zero_guess, int final) {
+  const unsigned zgrid = (unsigned) ((g.ninterior + zb - 1) / zb);
+  LaunchProfiler *pr = A.prof;
+
+  if (phase == PH_BEGIN) {
+    {
+      ProfScope ps(pr, st, KC_BEGIN, 1);
+      k_begin<<<1, 32, 0, st>>>(A.ctl, A.dt_mode, A.dt, A.cfl, A.min_dx);
+    }
+    ProfScope ps(pr, st, KC_P2C, g.ninterior);
+    k_prim_to_cons<T><<<zgrid, zb, 0, st>>>(g, cstate(b.Pc_bulk[0], b.Pc_B[0]), cstate(b.Pc_bulk[1], b.Pc_B[1]),
+                                            U0, A.pp.gamma, A.ctl);
+  } else if (phase == PH_C2P) {
+    // stage s < ns reads the stage input (U0 first, U1 after) into PA; s == ns is the
+    // closing c2p of U0 into the uncommitted primitive buffer
+    const int final = s == ns;
+    const StateCPtr<T> Uin = (s == 0 || final) ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B};
+    const int zero_guess = s == 0;
+    // learned guess on the tensor cores: persistent c2p kernel, MGPU_TC_CTAS_PER_SM CTAs per SM
+    // (4 x 128 threads x 128 registers fill the register file)
+    const bool tc_c2p = A.pp.learned && A.pp.mlp_tc;
+    const bool simt_net = A.pp.learned && A.pp.mlp && !A.pp.mlp_tc;   // per-thread network guess
+    const long long ntiles = (g.ninterior + 127) / 128;
+    const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
+    const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
+    ProfScope ps(pr, st, KC_C2P, g.ninterior);
     if (tc_c2p)
       k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
                                                                 final, A.ereset, A.preset, A.dreset);
@@ -45,35 +87,14 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
     else
       k_cons_to_prim<T, 2><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
           g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
-  };
-  const unsigned zgrid = (unsigned) ((g.ninterior + zb - 1) / zb);
-
-  LaunchProfiler *pr = A.prof;
-  {
-    ProfScope ps(pr, st, KC_BEGIN, 1);
-    k_begin<<<1, 32, 0, st>>>(A.ctl, A.dt_mode, A.dt, A.cfl, A.min_dx);
-  }
-  {
-    ProfScope ps(pr, st, KC_P2C, g.ninterior);
-    k_prim_to_cons<T><<<zgrid, zb, 0, st>>>(g, cstate(b.Pc_bulk[0], b.Pc_B[0]), cstate(b.Pc_bulk[1], b.Pc_B[1]),
-                                            U0, A.pp.gamma, A.ctl);
-  }
-  const int ns = num_stages(A.rk);
-  for (int s = 0; s < ns; ++s) {
-    const StatePtr<T> Uin = s == 0 ? U0 : U1;
-    {
-      ProfScope ps(pr, st, KC_C2P, g.ninterior);
-      c2p(StateCPtr<T>{Uin.bulk, Uin.B}, s, s == 0, 0);
-    }
+  } else if (phase == PH_FLUX_UPDATE) {
     for (int d = 1; d <= g.nd; ++d) {
       const long long S = g.s[d - 1];
       const long long nf = g.nz - 5 * S;
       if (nf <= 0) continue;
       const unsigned fgrid = (unsigned) ((nf + fb - 1) / fb);
       ProfScope ps(pr, st, KC_FLUX, nf);
-      if (d == 1) k_flux<T, 1><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[0], A.pp, A.ctl, s);
-      else if (d == 2) k_flux<T, 2><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[1], A.pp, A.ctl, s);
-      else k_flux<T, 3><<<fgrid, fb, 0, st>>>(g, PA, (T *) b.F[2], A.pp, A.ctl, s);
+      launch_flux<T>(g, d, A.pp.riemann, fgrid, fb, st, PA, (T *) b.F[d - 1], A.pp, A.ctl, s);
     }
     const StageKind kind = stage_kind(A.rk, s);
     UpdateArgs ua{kind.combine, kind.c};
@@ -95,16 +116,25 @@ inline cudaError_t launch_advance(const AdvanceArgs &A)
       k_update<T, 2><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
     else
       k_update<T, 3><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
-  }
-  {
-    ProfScope ps(pr, st, KC_C2P, g.ninterior);
-    c2p(StateCPtr<T>{U0.bulk, U0.B}, ns, 0, 1);
-  }
-  {
+  } else if (phase == PH_COMMIT) {
     ProfScope ps(pr, st, KC_BEGIN, 1);
     k_commit<<<1, 32, 0, st>>>(A.ctl, ns);
   }
   return cudaGetLastError();
+}
+
+template <class T>
+inline cudaError_t launch_advance(const AdvanceArgs &A)
+{
+  const int ns = num_stages(A.rk);
+  cudaError_t e = launch_phase<T>(A, PH_BEGIN, 0);
+  for (int s = 0; s < ns && e == cudaSuccess; ++s) {
+    e = launch_phase<T>(A, PH_C2P, s);
+    if (e == cudaSuccess) e = launch_phase<T>(A, PH_FLUX_UPDATE, s);
+  }
+  if (e == cudaSuccess) e = launch_phase<T>(A, PH_C2P, ns);
+  if (e == cudaSuccess) e = launch_phase<T>(A, PH_COMMIT, 0);
+  return e;
 }
 
 // AoS (host reference layout, 8 doubles per zone) <-> state arrays.
@@ -187,15 +217,82 @@ inline cudaError_t launch_face_io(const TransferArgs &A, double *d_aos, long lon
   return cudaGetLastError();
 }
 
+// ---- halo slabs of a decomposed domain ------------------------------------------------------
+// A slab is Ng layers of dimension `dim` over the full guarded cross-section of the other two
+// dimensions (so that exchanging dimensions in order x, y, z fills edges and corners as the
+// reference's sequential Synchronize does, Mara/subgrids.cpp:12-116).  Buffer layout:
+// [component][layer][cross-section index], the cross-section in zone order.
+__device__ __forceinline__ long long slab_zone(const Grid &g, int dim, int layer, long long c)
+{
+  if (dim == 0) return (long long) layer * g.s[0] + c;   // c = j*G2 + k
+  if (dim == 1) {                                        // c = i*G2 + k
+    const long long i = c / g.G[2], k = c - i * g.G[2];
+    return i * g.s[0] + (long long) layer * g.s[1] + k;
+  }
+  const long long i = c / g.G[1], j = c - i * g.G[1];   // c = i*G1 + j
+  return i * g.s[0] + j * g.s[1] + layer;
+}
+
+__host__ __device__ inline long long slab_cross(const Grid &g, int dim)
+{
+  return dim == 0 ? (long long) g.G[1] * g.G[2] : dim == 1 ? (long long) g.G[0] * g.G[2] : (long long) g.G[0] * g.G[1];
+}
+
+// to_buf 1: A[q][layers first..first+ng) -> buf; 0: buf -> A.  A has ncomp components of E.
+template <class E>
+__global__ void k_halo_copy(Grid g, E *A, int ncomp, int dim, int first, E *buf, int to_buf)
+{
+  const long long cross = slab_cross(g, dim);
+  const long long per = cross * g.ng;
+  const long long total = per * ncomp;
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long) gridDim.x * blockDim.x) {
+    const int q = (int) (t / per);
+    const long long r = t - q * per;
+    const int layer = (int) (r / cross);
+    const long long c = r - (long long) layer * cross;
+    const long long z = slab_zone(g, dim, first + layer, c);
+    if (to_buf) buf[t] = A[q * g.cs + z];
+    else A[q * g.cs + z] = buf[t];
+  }
+}
+
+// which 0: the stage primitives PA (8 x T); 1: the committed state (5 x T, then 3 x double).
+// side 0: the low slab (pack: interior layers [ng, 2ng) for the low neighbour; unpack: guard
+// layers [0, ng)); side 1: the high slab (pack: [n, n + ng); unpack: [n + ng, n + 2ng)).
+template <class T>
+inline cudaError_t launch_halo(const TransferArgs &A, int which, int dim, int side, void *buf, int pack)
+{
+  const Grid &g = A.g;
+  const int n = g.n[dim], ng = g.ng;
+  const int first = pack ? (side == 0 ? ng : n) : (side == 0 ? 0 : n + ng);
+  const long long per = slab_cross(g, dim) * ng;
+  const unsigned blk = 256;
+  const unsigned grid = (unsigned) std::min<long long>((per * 8 + blk - 1) / blk, 148ll * 16);
+  if (which == 0) {
+    k_halo_copy<T><<<grid, blk, 0, A.stream>>>(g, (T *) A.b.PA, 8, dim, first, (T *) buf, pack);
+  } else {
+    // the committed buffer is chosen on the host (it read ctl->cur after a synchronize)
+    const int cur = A.cur;
+    k_halo_copy<T><<<grid, blk, 0, A.stream>>>(g, (T *) A.b.Pc_bulk[cur], 5, dim, first, (T *) buf, pack);
+    k_halo_copy<double><<<grid, blk, 0, A.stream>>>(g, A.b.Pc_B[cur], 3, dim, first,
+                                                    (double *) ((char *) buf + per * 5 * sizeof(T)), pack);
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace mgpu
 
 #define MGPU_DEFINE_PRECISION(suffix, T)                                                                  \
   namespace mgpu {                                                                                       \
   cudaError_t advance_##suffix(const AdvanceArgs &A) { return launch_advance<T>(A); }                   \
+  cudaError_t phase_##suffix(const AdvanceArgs &A, int phase, int s) { return launch_phase<T>(A, phase, s); } \
   cudaError_t upload_##suffix(const TransferArgs &A, const double *d_aos, long long z0, long long count) \
   { return launch_upload<T>(A, d_aos, z0, count); }                                                      \
   cudaError_t download_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count)     \
   { return launch_download<T>(A, d_aos, z0, count); }                                                    \
   cudaError_t face_io_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count, int to_aos) \
   { return launch_face_io<T>(A, d_aos, z0, count, to_aos); }                                             \
+  cudaError_t halo_##suffix(const TransferArgs &A, int which, int dim, int side, void *buf, int pack)     \
+  { return launch_halo<T>(A, which, dim, side, buf, pack); }                                             \
   }

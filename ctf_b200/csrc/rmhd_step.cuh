@@ -19,9 +19,10 @@
 #ifndef MGPU_FLUX_MINB
 #define MGPU_FLUX_MINB 2
 #endif
-// The same for the zone c2p kernel (its natural register count allows 3 blocks).
+// The same for the zone c2p kernel (5 blocks: chosen by a sweep of 3-5; its natural register
+// count allows 3).
 #ifndef MGPU_C2P_MINB
-#define MGPU_C2P_MINB 3
+#define MGPU_C2P_MINB 5
 #endif
 
 namespace mgpu {
@@ -44,11 +45,25 @@ __device__ __forceinline__ int images_1d(int m, int n, int ng, bool active, int 
   return c;
 }
 
+// Whether dimension d (0-based) gets its guard layers from the periodic images of this
+// grid's own zones (false for unused dimensions and for dimensions whose guards a halo
+// exchange fills).
+__device__ __forceinline__ bool self_periodic(const Grid &g, int d) { return g.nd > d && !g.ext[d]; }
+
+// Number of guarded arrays holding zone (i, j, k) -- this grid's, counting the zone's
+// periodic images, and on a decomposed domain its neighbours' -- which is how many times
+// the reference's ConsToPrim over every guarded zone of every rank counts its failure
+// (Mara/hydro.cpp:133-149,201).
 __device__ __forceinline__ int multiplicity(const Grid &g, int i, int j, int k)
 {
   int p[3];
-  return images_1d(i, g.n[0], g.ng, g.nd >= 1, p) * images_1d(j, g.n[1], g.ng, g.nd >= 2, p) *
-         images_1d(k, g.n[2], g.ng, g.nd >= 3, p);
+  const int m[3] = {i, j, k};
+  int c = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (g.ext[d]) c *= g.mult[d][m[d] - g.ng];
+    else c *= images_1d(m[d], g.n[d], g.ng, g.nd > d, p);
+  }
+  return c;
 }
 
 template <class T>
@@ -151,9 +166,9 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
     }
   }
   int pi[3], pj[3], pk[3];
-  const int ni = images_1d(i, g.n[0], g.ng, g.nd >= 1, pi);
-  const int nj = images_1d(j, g.n[1], g.ng, g.nd >= 2, pj);
-  const int nk = images_1d(k, g.n[2], g.ng, g.nd >= 3, pk);
+  const int ni = images_1d(i, g.n[0], g.ng, self_periodic(g, 0), pi);
+  const int nj = images_1d(j, g.n[1], g.ng, self_periodic(g, 1), pj);
+  const int nk = images_1d(k, g.n[2], g.ng, self_periodic(g, 2), pk);
   for (int a = 0; a < ni; ++a)
     for (int b = 0; b < nj; ++b)
       for (int c = 0; c < nk; ++c) {
@@ -213,7 +228,7 @@ struct FluxTally {
 
 // One face: reconstruct, Riemann solve (PCM retry on failure), store the flux; the face's
 // |lambda| is folded into ml.
-template <class T, int dim>
+template <class T, int dim, int RS>
 __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ PA, T *__restrict__ F,
                                           const PhysParams &pp, long long f, T &ml, FluxTally &ft)
 {
@@ -239,7 +254,7 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
   T Fo[8];
   const T gamma = T(pp.gamma);
   int err = 1, used_hllc = 0;
-  const bool hlld = pp.riemann == RIEMANN_HLLD;
+  constexpr bool hlld = RS == RIEMANN_HLLD;
   C2PTally tally{0, 0};
   // attempt 0: reconstructed states; attempt 1: the zone states themselves (PCM retry).
   // One call site per solver keeps a single inlined copy of it.
@@ -254,8 +269,8 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
       }
     }
     C2PTally t{0, 0};
-    if (hlld) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
-    else if (pp.riemann == RIEMANN_HLLC) err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
+    if constexpr (RS == RIEMANN_HLLD) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
+    else if constexpr (RS == RIEMANN_HLLC) err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
     else err = riemann_hll<T, dim>(gamma, Pl, Pr, Fo, ml);
     tally.iters += t.iters;
     tally.attempts += t.attempts;
@@ -266,7 +281,7 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
   }
 #pragma unroll
   for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
-  if (hlld) {
+  if constexpr (hlld) {
     ft.hlld_ok += 1 - used_hllc;
     ft.hlld_hllc += used_hllc;
   }
@@ -300,7 +315,7 @@ __device__ __forceinline__ void flux_block_finish(double m, const FluxTally &ft,
   warp_add(&ctl->face_c2p_iters, (unsigned) ft.face_c2p_iters);
 }
 
-template <class T, int dim>
+template <class T, int dim, int RS>
 __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_flux(Grid g, const T *__restrict__ PA, T *__restrict__ F,
                                                               PhysParams pp, Ctl *ctl, int stage)
 {
@@ -309,8 +324,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_flux(Grid g, const T *_
   const long long f = 2 * S + (long long) blockIdx.x * blockDim.x + threadIdx.x;
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
-  if (f < g.nz - 3 * S) flux_face<T, dim>(g, PA, F, pp, f, ml, ft);
-  flux_block_finish(double(ml), ft, ctl, pp.riemann == RIEMANN_HLLD);
+  if (f < g.nz - 3 * S) flux_face<T, dim, RS>(g, PA, F, pp, f, ml, ft);
+  flux_block_finish(double(ml), ft, ctl, RS == RIEMANN_HLLD);
 }
 
 // ---- CT + flux divergence + Runge-Kutta combine ---------------------------------------------

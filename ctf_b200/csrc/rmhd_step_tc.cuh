@@ -53,41 +53,9 @@ __global__ void __launch_bounds__(128) k_cons_to_prim_tc(Grid g, StateCPtr<T> U,
     double Zg = 0.0, Wg = 0.0;
     const bool use = have && good && c2p_guess_from_output(u[ddd], y, Zg, Wg);
     C2PTally tally;
-    int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
-    warp_add(&ctl->c2p_calls, 1u);
-    warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
-    if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
-    if (err) {
-      if (ereset) {
-        p[0] = dreset;
-        p[1] = preset;
-        p[2] = p[3] = p[4] = 0.0;
-        p[5] = u[5];
-        p[6] = u[6];
-        p[7] = u[7];
-      } else {
-        atomicAdd(final ? &ctl->final_err : &ctl->stage_err[stage], multiplicity(g, i, j, k));
-      }
-    }
-    int pi[3], pj[3], pk[3];
-    const int ni = images_1d(i, g.n[0], g.ng, g.nd >= 1, pi);
-    const int nj = images_1d(j, g.n[1], g.ng, g.nd >= 2, pj);
-    const int nk = images_1d(k, g.n[2], g.ng, g.nd >= 3, pk);
-    StatePtr<T> Pn = ctl->cur ? Pn0 : Pn1;
-    for (int a = 0; a < ni; ++a)
-      for (int b = 0; b < nj; ++b)
-        for (int c = 0; c < nk; ++c) {
-          const long long w = ((long long) pi[a] * g.G[1] + pj[b]) * g.G[2] + pk[c];
-          if (final) {
-#pragma unroll
-            for (int q = 0; q < 5; ++q) Pn.bulk[q * g.cs + w] = T(p[q]);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) Pn.B[q * g.cs + w] = p[5 + q];
-          } else {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) PA[q * g.cs + w] = T(p[q]);
-          }
-        }
+    const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
+    c2p_finish<T>(g, PA, ctl->cur ? Pn0 : Pn1, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err,
+                  tally);
   }
   if (!net.ok && threadIdx.x == 0) atomicExch(&ctl->tc_fault, 1);
   tc::tc_teardown(net);

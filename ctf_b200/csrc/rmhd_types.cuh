@@ -59,6 +59,11 @@ struct Grid {
   long long s[3]; // zone strides of x, y, z
   double dx, dy, dz;
   long long ninterior;
+  // Decomposed domains: ext[d] = 1 when a halo exchange fills the guard layers of dimension
+  // d (the c2p then scatters no periodic images along d), and mult[d][m] is the number of
+  // guarded arrays, over all ranks, that hold interior index m of d (device, n[d] entries).
+  int ext[3];
+  const int *mult[3];
 };
 
 template <class T> struct StatePtr {   // components 0..4 in T, 5..7 in double
@@ -167,6 +172,7 @@ struct TransferArgs {
   AdvanceBuffers b;
   Ctl *ctl;
   cudaStream_t stream;
+  int cur;   // committed buffer, for the halo copies of the committed state
 };
 
 // One member of an ensemble of boxes (device-side descriptor).
@@ -204,9 +210,11 @@ struct EnsembleArgs {
 #define MGPU_DECLARE_PRECISION(suffix)                                                                   \
   namespace mgpu {                                                                                       \
   cudaError_t advance_##suffix(const AdvanceArgs &A);                                                    \
+  cudaError_t phase_##suffix(const AdvanceArgs &A, int phase, int s);                                    \
   cudaError_t upload_##suffix(const TransferArgs &A, const double *d_aos, long long z0, long long count); \
   cudaError_t download_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count);     \
   cudaError_t face_io_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count, int to_aos); \
+  cudaError_t halo_##suffix(const TransferArgs &A, int which, int dim, int side, void *buf, int pack);   \
   cudaError_t ensemble_advance_##suffix(const EnsembleArgs &E);                                          \
   }
 

@@ -155,6 +155,31 @@ int mgpu_mlp_forward_tc(const float *params, const float *dev_x, long long n, fl
 int mgpu_mlp_tc_image_bytes(void);
 int mgpu_mlp_build_tc_image(const float *params, void *image);
 
+/* ---- domain decomposition (the reference's DecomposedCartesianDomain with MPI,
+ * Mara/subgrids.cpp:12-147, Mara/mara_mpi.c:96-130; here any transport, e.g. NCCL) --------
+ * A rank's solver holds its subdomain (mgpu_set_domain with the local x0, x1, N).  For every
+ * dimension split across ranks, mgpu_set_external_guards turns off the periodic guard fill
+ * and takes multiplicity tables: mult lists, for each such dimension in order and each
+ * local interior index along it, how many guarded arrays over all ranks hold that zone (the
+ * reference counts a failed zone once per array holding it, Mara/hydro.cpp:133-149,201).
+ * The host then drives each advance phase by phase and fills the guards between them:
+ *   mgpu_advance_phase(0 begin) ; per stage s: phase(1 c2p, s), exchange the stage
+ *   primitives (which 0) for every split dimension in order x, y, z with
+ *   mgpu_halo_pack / mgpu_halo_unpack, phase(2 flux+update, s) ; phase(1 c2p, stages) ;
+ *   sum the five error counters and max the MaxLambda bits (mgpu_reduction_targets, device
+ *   memory: int[5] = stage 1-4 and closing c2p, uint64 = a non-negative double's bits) over
+ *   all ranks ; phase(3 commit).
+ * Slabs are Ng layers over the full guarded cross-section (edges and corners follow from
+ * the x, y, z order); side 0 packs the low interior layers / unpacks the low guards, side 1
+ * the high ones.  which 1 exchanges the committed state (before a download with guards).
+ * Asynchronous on the handle's stream except where noted. */
+int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double dt, double cfl);
+int mgpu_reduction_targets(mgpu_solver *h, void **err_counts, void **max_lambda_bits);
+int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult);   /* synchronous */
+int mgpu_halo_bytes(mgpu_solver *h, int which, int dim, long long *bytes);
+int mgpu_halo_pack(mgpu_solver *h, int which, int dim, int side, void *dev_buf);
+int mgpu_halo_unpack(mgpu_solver *h, int which, int dim, int side, const void *dev_buf);
+
 /* Allocation-free advance (no counterpart in the reference).  For callers that may not
  * allocate device memory -- allocation-free sections of a larger application, real-time
  * loops, hosts that hand out only pre-owned buffers: one FP64 advance of a box of at most

@@ -45,6 +45,10 @@ WORKLOADS = {
                              dict(extrap="plm", riemann="hlld", advance="rk3")),
     "turb128_weno5_hlld_rk3": ((128, 128, 128), "turbulence",
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
+    # profiling size: the face array (166^3 x 8 x 4 B = 146 MB) still exceeds the 126 MB L2
+    "turb160_weno5_hlld_rk3": ((160, 160, 160), "turbulence",
+                               dict(extrap="weno5", riemann="hlld", advance="rk3")),
+    "stress512_plm_hlld_rk3": ((512, 512, 512), "stress", dict(extrap="plm", riemann="hlld", advance="rk3")),
 }
 DEFAULT_WORKLOAD = "turb256_weno5_hlld_rk3"
 # ensembles: 256 independent 2D Kelvin-Helmholtz boxes, sides log-uniform in 64..512
@@ -462,6 +466,7 @@ def main():
         runs.append(("fp32", True))
     results, states, solvers = {}, {}, {}
     dt_fixed = None
+    head_key = "fp32+learned" if net is not None else "fp32"
     for prec, learned in runs:
         key = prec + ("+learned" if learned else "")
         s = Solver(Scheme(precision=prec, learned_c2p=learned, **scheme_kw), n, stream=stream.cuda_stream)
@@ -487,14 +492,14 @@ def main():
         results[key] = {"ms_total": ms, "ms_per_step": ms / args.steps,
                         "value": zones * args.steps * world / (ms * 1e-3), "prof": prof, "stats": st,
                         "clocks": clk.summary()}
-        states[key] = s.download()
+        st_out = s.download()
+        states[key] = st_out if key in ("fp64", head_key) else None
         s.profile_disable()
-        solvers[key] = s
-    head_key = "fp32+learned" if "fp32+learned" in results else "fp32"
+        if key == head_key:
+            solvers[key] = s
+        else:
+            s.close()   # one solver on the device at a time (512^3 FP64 alone holds 71 GB)
     solver_fp32 = solvers[head_key]
-    for k, s in solvers.items():
-        if k != head_key:
-            s.close()
 
     head = results[head_key]
     out = {
@@ -539,8 +544,15 @@ def main():
     alg_bytes_per_launch = per_unit[dom] * d["units"] / max(d["launches"], 1)
     avg_ms = d["ms"] / max(d["launches"], 1)
     achieved = alg_bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    # DRAM bytes per work unit from one ncu capture of the same kernel on the 160^3 box of
+    # this scheme (profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md,
+    # profiles/k_update_turb160_weno5_hlld_rk3_fp32.md), scaled to this launch's units
+    measured = {("flux", "hlld"): 72.8, ("update", "hlld"): 220.2}
+    tpu = measured.get((dom, scheme_kw["riemann"])) if head_key.startswith("fp32") else None
+    traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                       "frac": achieved / hbm, "traffic": None,
+                       "frac": achieved / hbm, "traffic": traffic,
+                       "traffic_source": "ncu dram__bytes_read+write per unit at 160^3, scaled" if tpu else None,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
                        "algorithmic_bytes_per_unit": per_unit[dom]}

@@ -51,7 +51,11 @@ template <> struct RmhdTol<float> {
   static constexpr float degenerate = 1e-6f;
   static constexpr float bx_small = 1e-6f;
   static constexpr float bjump = 1e-6f;
+#ifdef MGPU_HLLC_BX_F32
+  static constexpr float hllc_bx = MGPU_HLLC_BX_F32;
+#else
   static constexpr float hllc_bx = 1e-7f;
+#endif
   static constexpr float hllc_a = 1e-6f;
 };
 
@@ -676,16 +680,26 @@ __device__ __forceinline__ int riemann_hll(T gamma, const T *Pl, const T *Pr, T 
 }
 
 // Contact speed of HLLC: the root (-b - sqrt(b^2 - 4ac)) / (2a) of a x^2 + b x + c, or -c/b
-// when |a| is below SMALL_A (Mara/riemann_hllc-rmhd.cpp:96,134); evaluated in FP64 for both
-// precisions (the FP32 path computes the star state in FP64, see riemann_hllc).
+// when |a| is below SMALL_A (Mara/riemann_hllc-rmhd.cpp:96,134).  In FP64 the reference's
+// expression is kept as written.  In FP32 it cancels catastrophically when a is small and
+// b < 0 (an error of ~eps * |b| / a), so the FP32 path uses the algebraically identical
+// 2c / (-b + sqrt(b^2 - 4ac)) there.
 template <class T>
 __device__ __forceinline__ T hllc_contact_speed(T a, T b, T c)
 {
   using Tol = RmhdTol<T>;
   if (m_abs(a) < T(Tol::hllc_a)) return -c / b;
-  return (-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a);
+  if (sizeof(T) == sizeof(double)) return (-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a);
+  const T sq = m_sqrt(b * b - T(4) * a * c);
+  return b <= T(0) ? T(2) * c / (-b + sq) : -(b + sq) / (T(2) * a);
 }
 
+// The HLL average, the HLLC star states and the flux at s = 0 from the two sides' states,
+// fluxes (total-energy convention) and the outer speeds.  `safeguard` (the FP32 path): a
+// non-finite contact speed or star state -- which FP32 overflow or a vanishing FP32
+// denominator can produce where FP64 stays finite -- takes the HLL flux instead.  Star
+// states that are merely unphysical (negative pressure, superluminal contact) are kept, as
+// the reference keeps them, so the two precisions take the same branch.
 template <class C, int dim>
 __device__ __forceinline__ void hllc_star_flux(const C *Pl, const C *Pr, const C *Ul, const C *Ur, const C *Fl,
                                                const C *Fr, C ap, C am, C *F, bool safeguard)
@@ -754,8 +768,9 @@ __device__ __forceinline__ void hllc_star_flux(const C *Pl, const C *Pr, const C
   }
   const T s = T(0);
   if (safeguard) {
-    const bool bad = !(isfinite(lc) && m_abs(lc) < T(1) && hllc_star_p >= T(0) && Ul_[ddd] > T(0) &&
-                       Ur_[ddd] > T(0) && isfinite(Ul_[tau]) && isfinite(Ur_[tau]));
+    bool bad = !(isfinite(lc) && isfinite(hllc_star_p));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) bad = bad || !isfinite(Ul_[i]) || !isfinite(Ur_[i]);
     if (bad) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) F[i] = (s <= am) ? Fl[i] : (s <= ap ? Fh[i] : Fr[i]);
@@ -774,46 +789,12 @@ __device__ __forceinline__ void hllc_star_flux(const C *Pl, const C *Pr, const C
 }
 
 
-// HllcRmhdRiemannSolver::IntercellFlux at s = 0 (Mara/riemann_hllc-rmhd.cpp:26-178).
-// FP64: the reference's arithmetic throughout.  FP32 faces: the fast speeds (the quartic) in
-// FP32, but the side states, their fluxes and the star state in FP64 -- the transverse
-// contact velocities (F_hll[B2] - U_hll[B2] w1) / U_hll[B1] cancel catastrophically where the
-// normal field is weak, which in FP32 costs ~1e-4 of the flow (measured on the 3D turbulence
-// box); in FP64 that cancellation is harmless.
+// HllcRmhdRiemannSolver::IntercellFlux at s = 0 (Mara/riemann_hllc-rmhd.cpp:26-178)
 template <class T, int dim>
 __device__ __forceinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T *F, T &ml)
 {
   using M = DimMap<dim>;
   constexpr int B1 = M::B1;
-  if constexpr (sizeof(T) < sizeof(double)) {
-    double Pl[8], Pr[8], Ul[8], Ur[8], Fl[8], Fr[8], dummy;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) { Pl[i] = double(pl[i]); Pr[i] = double(pr[i]); }
-    Pl[B1] = Pr[B1] = 0.5 * (Pl[B1] + Pr[B1]);
-    const double gd = double(gamma);
-    if (prim_to_cons(gd, Pl, Ul)) return 1;
-    if (prim_to_cons(gd, Pr, Ur)) return 1;
-    flux_and_eigenvalues(gd, Ul, Pl, Fl, dummy, dummy, dim, false);
-    flux_and_eigenvalues(gd, Ur, Pr, Fr, dummy, dummy, dim, false);
-    T Plf[8], Prf[8], Ulf[8], Urf[8], Flf[8], Frf[8], epl, eml, epr, emr;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      Plf[i] = T(Pl[i]); Prf[i] = T(Pr[i]); Ulf[i] = T(Ul[i]); Urf[i] = T(Ur[i]);
-    }
-    flux_and_eigenvalues(gamma, Ulf, Plf, Flf, epl, eml, dim);   // speeds only are used
-    flux_and_eigenvalues(gamma, Urf, Prf, Frf, epr, emr, dim);
-    Ul[tau] += Ul[ddd]; Fl[tau] += Fl[ddd];
-    Ur[tau] += Ur[ddd]; Fr[tau] += Fr[ddd];
-    const T ap = (epl > epr) ? epl : epr;
-    const T am = (eml < emr) ? eml : emr;
-    const T l = face_lambda(ap, am);
-    if (ml < l) ml = l;
-    double Fd[8];
-    hllc_star_flux<double, dim>(Pl, Pr, Ul, Ur, Fl, Fr, double(ap), double(am), Fd, true);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) F[i] = T(Fd[i]);
-    return 0;
-  } else {
   T Pl[8], Pr[8], Ul[8], Ur[8], Fl[8], Fr[8], epl, eml, epr, emr;
 #pragma unroll
   for (int i = 0; i < 8; ++i) { Pl[i] = pl[i]; Pr[i] = pr[i]; }
@@ -828,9 +809,8 @@ __device__ __forceinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T
   const T am = (eml < emr) ? eml : emr;
   const T l = face_lambda(ap, am);
   if (ml < l) ml = l;
-  hllc_star_flux<T, dim>(Pl, Pr, Ul, Ur, Fl, Fr, ap, am, F, false);
+  hllc_star_flux<T, dim>(Pl, Pr, Ul, Ur, Fl, Fr, ap, am, F, sizeof(T) < sizeof(double));
   return 0;
-  }
 }
 
 // Out-of-line HLLC for the HLLD fallback (rare): arguments and result by value so that the

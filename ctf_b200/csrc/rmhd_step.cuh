@@ -444,8 +444,11 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
   }
 }
 
+#ifndef MGPU_UPDATE_MINB
+#define MGPU_UPDATE_MINB 1
+#endif
 template <class T, int ND>
-__global__ void __launch_bounds__(256) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
+__global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
                                                 const T *__restrict__ F, const T *__restrict__ G,
                                                 const T *__restrict__ H, StatePtr<T> Uout, StatePtr<T> Kout,
                                                 StateCPtr<T> K1, StateCPtr<T> K2, StateCPtr<T> K3,

@@ -536,10 +536,16 @@ def main():
     prof = head["prof"]
     dom = max(("flux", "update", "c2p", "p2c"), key=lambda k: prof[k]["ms"])
     tsz = 4
+    nd = len(n)
+    ns = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}[scheme_kw["advance"]]
+    state = 5 * tsz + 3 * 8                             # 44 B: FP32 bulk + FP64 B
+    # update: read U^n (+ U^(s) after the first stage), the nd fluxes; write the new state --
+    # averaged over the stages (RK4's K registers are not counted)
+    upd = (state * (2 * ns + (ns - 1)) + ns * nd * 8 * tsz) / ns
     per_unit = {"flux": 16 * tsz,                       # read 8 face-state comps, write 8 flux comps
-                "update": 5 * tsz * 3 + 3 * 8 * 3 + 3 * 8 * tsz,   # Un, Us, Uout (44 B each) + F,G,H
-                "c2p": 44 + 8 * tsz,                    # read U (44 B), write 8 prim comps
-                "p2c": 44 + 44}
+                "update": upd,
+                "c2p": state + 8 * tsz,                 # read U, write 8 prim comps (interior)
+                "p2c": 2 * state}
     d = prof[dom]
     alg_bytes_per_launch = per_unit[dom] * d["units"] / max(d["launches"], 1)
     avg_ms = d["ms"] / max(d["launches"], 1)
@@ -556,6 +562,14 @@ def main():
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
                        "algorithmic_bytes_per_unit": per_unit[dom]}
+    # every kernel class against the HBM roofline (algorithmic bytes / event-timed duration)
+    out["kernels"] = {}
+    for k in ("flux", "update", "c2p", "p2c"):
+        pk = prof[k]
+        if pk["launches"] and pk["ms"] > 0:
+            gbs = per_unit[k] * pk["units"] / (pk["ms"] * 1e-3) / 1e9
+            out["kernels"][k] = {"ms_per_launch": pk["ms"] / pk["launches"], "bytes_per_unit": per_unit[k],
+                                 "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / hbm}
     out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "c2p_attempt", "face_c2p_calls",
                                                       "face_c2p_iters", "hlld_ok", "hlld_hllc", "pcm_retry")}
 

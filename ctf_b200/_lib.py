@@ -99,6 +99,14 @@ SIGNATURES = {
     "mgpu_halo_bytes": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
     "mgpu_halo_pack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "mgpu_halo_unpack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "mgpu_new_ou_field": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         _vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_set_driving": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong]),
+    "mgpu_driving_advance": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "mgpu_driving_resample": (ctypes.c_int, [_vp]),
+    "mgpu_driving_serialize": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "mgpu_driving_power": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_ou_field_advance": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_double]),
     "mgpu_ensemble_create": (ctypes.c_int, [ctypes.POINTER(MgpuConfig), ctypes.c_int, ctypes.c_int, _ip, _dp, _dp,
                                             ctypes.POINTER(_vp)]),
     "mgpu_ensemble_destroy": (ctypes.c_int, [_vp]),

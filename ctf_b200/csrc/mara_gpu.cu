@@ -17,37 +17,7 @@ MGPU_DECLARE_PRECISION(fp32)
 
 using namespace mgpu;
 
-struct mgpu_solver {
-  mgpu_config cfg;
-  std::string err;
-  bool have_domain = false;
-  Grid g{};
-  double x0[3] = {0, 0, 0}, x1[3] = {1, 1, 1};
-  double min_dx = 1.0;
-  int N[3] = {1, 1, 1};
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int device = 0;
-  AdvanceBuffers b{};
-  std::vector<void *> allocations;
-  Ctl *ctl = nullptr;           // device
-  Ctl *ctl_host = nullptr;      // pinned mirror
-  double *staging = nullptr;    // device AoS staging for host transfers
-  long long staging_zones = 0;
-  double *red = nullptr;        // reduction partials (device)
-  double *red_host = nullptr;   // pinned
-  float *mlp = nullptr;         // learned c2p network (device)
-  long long mlp_count = 0;
-  void *mlp_tc = nullptr;       // its tensor-core image (device)
-  int *mult = nullptr;          // multiplicity tables of a decomposed domain (device)
-  // kernel timing
-  std::vector<cudaEvent_t> prof_ev;
-  std::vector<int> prof_tag;
-  std::vector<long long> prof_units;
-  int prof_count = 0;
-  LaunchProfiler prof{};
-  bool prof_on = false;
-};
+#include "solver.h"
 
 namespace {
 
@@ -300,6 +270,7 @@ int mgpu_destroy(mgpu_solver *h)
 {
   if (!h) return MGPU_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  mgpu_driving_free(h);
   free_buffers(h);
   prof_free(h);
   if (h->mlp) cudaFree(h->mlp);
@@ -340,6 +311,7 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
     if (N[d] < ng) return fail(h, MGPU_ERR_ARG, "periodic guard fill needs N >= Ng on every axis");
   CK(cudaStreamSynchronize(h->stream));
   free_buffers(h);
+  mgpu_driving_free(h);
   if (h->mult) cudaFree(h->mult);
   h->mult = nullptr;
   h->have_domain = false;
@@ -499,6 +471,7 @@ static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
   A.prof = h->prof_on ? &h->prof : nullptr;
   cudaError_t e = fp32(h) ? advance_fp32(A) : advance_fp64(A);
   CK(e);
+  CK(mgpu_driving_enqueue(h));
   return MGPU_OK;
 }
 
@@ -742,6 +715,7 @@ int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double
   A.stream = h->stream;
   A.prof = h->prof_on ? &h->prof : nullptr;
   CK(fp32(h) ? phase_fp32(A, phase, stage) : phase_fp64(A, phase, stage));
+  if (phase == 3) CK(mgpu_driving_enqueue(h));
   return MGPU_OK;
 }
 

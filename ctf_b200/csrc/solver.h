@@ -1,0 +1,49 @@
+// The solver handle behind the C ABI (shared by the host translation units of libmaragpu.so).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+
+#include "../../include/mara_gpu.h"
+#include "rmhd_types.cuh"
+
+struct MgpuDriving;   // OU driving field (driving.cu)
+
+struct mgpu_solver {
+  mgpu_config cfg;
+  std::string err;
+  bool have_domain = false;
+  mgpu::Grid g{};
+  double x0[3] = {0, 0, 0}, x1[3] = {1, 1, 1};
+  double min_dx = 1.0;
+  int N[3] = {1, 1, 1};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  mgpu::AdvanceBuffers b{};
+  std::vector<void *> allocations;
+  mgpu::Ctl *ctl = nullptr;           // device
+  mgpu::Ctl *ctl_host = nullptr;      // pinned mirror
+  double *staging = nullptr;    // device AoS staging for host transfers
+  long long staging_zones = 0;
+  double *red = nullptr;        // reduction partials (device)
+  double *red_host = nullptr;   // pinned
+  float *mlp = nullptr;         // learned c2p network (device)
+  long long mlp_count = 0;
+  void *mlp_tc = nullptr;       // its tensor-core image (device)
+  int *mult = nullptr;          // multiplicity tables of a decomposed domain (device)
+  MgpuDriving *driving = nullptr;   // velocity forcing applied after each committed advance
+  // kernel timing
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_tag;
+  std::vector<long long> prof_units;
+  int prof_count = 0;
+  mgpu::LaunchProfiler prof{};
+  bool prof_on = false;
+};
+
+
+// Enqueues the driving kick of the just-committed state (no-op without a driving field or
+// when the advance did not commit); defined in driving.cu.
+cudaError_t mgpu_driving_enqueue(mgpu_solver *h);
+void mgpu_driving_free(mgpu_solver *h);

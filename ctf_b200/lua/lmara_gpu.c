@@ -45,6 +45,8 @@ typedef struct {
   long long nzones;
   float *net;                /* learned c2p parameters (host copy) */
   long long net_count;
+  char *drive;               /* driving field carried across a solver rebuild */
+  long long drive_len;
 } MaraGpu;
 
 static MaraGpu M;
@@ -66,6 +68,16 @@ static mgpu_solver *solver(lua_State *L)
   if (!M.started) luaL_error(L, "[Mara] call Mara.start() first");
   if (!M.have_domain) luaL_error(L, "[Mara] need a domain to run this, use set_domain");
   if (M.h && !M.dirty) return M.h;
+  if (M.h) {   /* keep the driving field (its OU state) across the rebuild */
+    long long n = 0;
+    free(M.drive);
+    M.drive = NULL;
+    M.drive_len = 0;
+    if (mgpu_driving_serialize(M.h, NULL, &n) == 0 && n > 0 && (M.drive = (char *) malloc((size_t) n))) {
+      mgpu_driving_serialize(M.h, M.drive, &n);
+      M.drive_len = n;
+    }
+  }
   free_solver();
   int rc = mgpu_create(&M.cfg, &M.h);
   if (rc) {
@@ -77,6 +89,10 @@ static mgpu_solver *solver(lua_State *L)
   if (M.net) {
     rc = mgpu_set_c2p_network(M.h, M.net, M.net_count);
     if (rc) raise_abi(L, rc, "set_c2p_network");
+  }
+  if (M.drive) {
+    rc = mgpu_set_driving(M.h, M.drive, M.drive_len);
+    if (rc) raise_abi(L, rc, "set_driving");
   }
   M.dirty = 0;
   return M.h;
@@ -118,6 +134,7 @@ static int l_start(lua_State *L)
   free_solver();
   free(M.prim);
   free(M.net);
+  free(M.drive);
   memset(&M, 0, sizeof(M));
   mgpu_default_config(&M.cfg);
   if (had) {
@@ -137,6 +154,7 @@ static int l_close(lua_State *L)
   free_solver();
   free(M.prim);
   free(M.net);
+  free(M.drive);
   memset(&M, 0, sizeof(M));
   return 0;
 }
@@ -353,6 +371,9 @@ static int l_set_domain(lua_State *L)
     M.nzones *= d < nd ? M.N[d] + 2 * ng : 1;
   }
   free(M.prim);
+  free(M.drive);
+  M.drive = NULL;
+  M.drive_len = 0;
   M.prim = (double *) calloc((size_t) (M.nzones * nq), sizeof(double));
   if (!M.prim) return luaL_error(L, "[Mara] out of host memory");
   M.have_domain = 1;
@@ -445,6 +466,74 @@ static int l_set_c2p_network(lua_State *L)
   return 0;
 }
 
+/* ---- driving (Mara.new_ou_field, Mara.set_driving, Mara.driving.*; mara.cpp:1169-1190,
+ * 1378-1401, 1771-1808): the reference's serialized fields, as Lua strings ------------------ */
+static int l_new_ou_field(lua_State *L)
+{
+  const int nd = (int) luaL_checkinteger(L, 1);
+  const double P0 = luaL_checknumber(L, 2), zeta = luaL_checknumber(L, 3);
+  const int k1 = (int) luaL_checkinteger(L, 4), seed = (int) luaL_checkinteger(L, 5);
+  long long n = 0;
+  if (mgpu_new_ou_field(nd, P0, zeta, k1, seed, NULL, &n)) return luaL_error(L, "[Mara] bad new_ou_field arguments");
+  char *buf = (char *) malloc((size_t) n);
+  if (!buf) return luaL_error(L, "[Mara] out of host memory");
+  mgpu_new_ou_field(nd, P0, zeta, k1, seed, buf, &n);
+  lua_pushlstring(L, buf, (size_t) n);
+  free(buf);
+  return 1;
+}
+
+static int l_set_driving(lua_State *L)
+{
+  size_t len = 0;
+  const char *f = luaL_checklstring(L, 1, &len);
+  const int rc = mgpu_set_driving(solver(L), f, (long long) len);
+  if (rc) return raise_abi(L, rc, "set_driving");
+  return 0;
+}
+
+static int l_driving_advance(lua_State *L)
+{
+  const int rc = mgpu_driving_advance(solver(L), luaL_checknumber(L, 1));
+  if (rc) return raise_abi(L, rc, "driving.Advance");
+  return 0;
+}
+
+static int l_driving_resample(lua_State *L)
+{
+  const int rc = mgpu_driving_resample(solver(L));
+  if (rc) return raise_abi(L, rc, "driving.Resample");
+  return 0;
+}
+
+static int l_driving_serialize(lua_State *L)
+{
+  long long n = 0;
+  mgpu_solver *h = solver(L);
+  int rc = mgpu_driving_serialize(h, NULL, &n);
+  if (rc) return raise_abi(L, rc, "driving.Serialize");
+  if (n == 0) return 0;   /* no driving: nothing, as the reference */
+  char *buf = (char *) malloc((size_t) n);
+  if (!buf) return luaL_error(L, "[Mara] out of host memory");
+  rc = mgpu_driving_serialize(h, buf, &n);
+  if (rc) {
+    free(buf);
+    return raise_abi(L, rc, "driving.Serialize");
+  }
+  lua_pushlstring(L, buf, (size_t) n);
+  free(buf);
+  return 1;
+}
+
+static int l_driving_power(lua_State *L)
+{
+  double p = 0.0;
+  const int rc = mgpu_driving_power(solver(L), &p);
+  if (rc) return raise_abi(L, rc, "driving.Power");
+  lua_pushnumber(L, p);
+  return 1;
+}
+
 static int l_gpu_stats(lua_State *L)
 {
   mgpu_stats s;
@@ -535,11 +624,13 @@ int luaopen_Mara(lua_State *L)
       {"set_primitive", l_set_primitive},
       {"config_solver", l_config_solver},
       {"set_c2p_network", l_set_c2p_network},
+      {"new_ou_field", l_new_ou_field},
+      {"set_driving", l_set_driving},
       {"gpu_stats", l_gpu_stats},
       {NULL, NULL}};
   static const char *const absent[] = {"show", "diffuse", "set_failmask", "prim_at_point", "set_units",
-                                       "set_driving", "set_cooling", "set_fluxsrc", "set_srcterm",
-                                       "cooling_rate", "new_ou_field", "load_shen", "test_shen",
+                                       "set_cooling", "set_fluxsrc", "set_srcterm",
+                                       "cooling_rate", "load_shen", "test_shen",
                                        "test_rmhd_c2p", "test_sampling", "test_sampling_many", NULL};
   static const luaL_Reg measure[] = {{"mean_max_divB", l_mean_max_divB},
                                      {"max_lorentz_factor", l_max_lorentz_factor},
@@ -564,7 +655,16 @@ int luaopen_Mara(lua_State *L)
   register_absent(L, fluid_absent);
   lua_setfield(L, -2, "fluid");
 
-  static const char *const sub[] = {"eos", "units", "driving", "image", "models", NULL};
+  static const luaL_Reg driving[] = {{"Advance", l_driving_advance},
+                                     {"Resample", l_driving_resample},
+                                     {"Serialize", l_driving_serialize},
+                                     {"Power", l_driving_power},
+                                     {NULL, NULL}};
+  lua_newtable(L);
+  luaL_setfuncs(L, driving, 0);
+  lua_setfield(L, -2, "driving");
+
+  static const char *const sub[] = {"eos", "units", "image", "models", NULL};
   for (const char *const *s = sub; *s; ++s) {
     lua_newtable(L);
     lua_setfield(L, -2, *s);

@@ -224,6 +224,44 @@ class Solver:
         self._check(self.lib.mgpu_set_c2p_network(
             self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size))
 
+    # ---- stochastic driving (Mara.set_driving / Mara.driving.*) ----------------------------
+    def set_driving(self, field: bytes | None):
+        """A serialized OU driving field (new_ou_field, or a checkpoint's); None clears it."""
+        if field is None:
+            self._check(self.lib.mgpu_set_driving(self.h, None, 0))
+            return
+        buf = ctypes.create_string_buffer(bytes(field), len(field))
+        self._check(self.lib.mgpu_set_driving(self.h, buf, len(field)))
+
+    def driving_advance(self, dt: float):
+        self._check(self.lib.mgpu_driving_advance(self.h, float(dt)))
+
+    def driving_resample(self):
+        self._check(self.lib.mgpu_driving_resample(self.h))
+
+    def driving_serialize(self) -> bytes:
+        n = ctypes.c_longlong()
+        self._check(self.lib.mgpu_driving_serialize(self.h, None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(max(n.value, 1))
+        self._check(self.lib.mgpu_driving_serialize(self.h, buf, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def driving_power(self) -> float:
+        p = ctypes.c_double()
+        self._check(self.lib.mgpu_driving_power(self.h, ctypes.byref(p)))
+        return p.value
+
+
+def new_ou_field(nd: int, P0: float, zeta: float, k1: int, seed: int) -> bytes:
+    """Mara.new_ou_field (Mara/mara.cpp:1378-1401): a serialized OU driving field."""
+    lib = _lib.load()
+    n = ctypes.c_longlong()
+    if lib.mgpu_new_ou_field(nd, float(P0), float(zeta), k1, seed, None, ctypes.byref(n)):
+        raise MaraError("[Mara] bad new_ou_field arguments")
+    buf = ctypes.create_string_buffer(n.value)
+    lib.mgpu_new_ou_field(nd, float(P0), float(zeta), k1, seed, buf, ctypes.byref(n))
+    return buf.raw
+
 
 class _Measure:
     def __init__(self, mod):

@@ -155,6 +155,23 @@ int mgpu_mlp_forward_tc(const float *params, const float *dev_x, long long n, fl
 int mgpu_mlp_tc_image_bytes(void);
 int mgpu_mlp_build_tc_image(const float *params, void *image);
 
+/* ---- stochastic driving (Mara.new_ou_field / set_driving / driving.*, Mara/mara.cpp:1169-1190,
+ * 1378-1401, 1771-1808; Mara/ou-field.cpp, Mara/driving.cpp) ---------------------------------
+ * A driving field is the reference's serialized StochasticVectorField (the bytes
+ * Mara.new_ou_field returns and Mara.driving.Serialize writes to checkpoints): mode
+ * amplitudes and their OU random streams.  While a solver holds one, every advance that
+ * commits kicks the 4-velocity of every zone by F dt / W (rest mass per zone kept) --
+ * DrivingProcedure::Drive_rmhd.  Two-call pattern for sizes: out NULL -> *bytes. */
+int mgpu_new_ou_field(int nd, double P0, double zeta, int k1, int seed, void *out, long long *bytes);
+/* replaces luaC_set_driving; field NULL clears it.  Samples the field on the grid. */
+int mgpu_set_driving(mgpu_solver *h, const void *field, long long bytes);
+int mgpu_driving_advance(mgpu_solver *h, double dt);      /* Mara.driving.Advance(dt): OU step */
+int mgpu_driving_resample(mgpu_solver *h);                /* Mara.driving.Resample() */
+int mgpu_driving_serialize(mgpu_solver *h, void *out, long long *bytes);   /* Mara.driving.Serialize() */
+int mgpu_driving_power(mgpu_solver *h, double *power);    /* Mara.driving.Power() */
+/* The OU step of a serialized field in place, without a solver (host only). */
+int mgpu_ou_field_advance(void *field, long long bytes, int nd, double dt);
+
 /* ---- domain decomposition (the reference's DecomposedCartesianDomain with MPI,
  * Mara/subgrids.cpp:12-147, Mara/mara_mpi.c:96-130; here any transport, e.g. NCCL) --------
  * A rank's solver holds its subdomain (mgpu_set_domain with the local x0, x1, N).  For every

@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256, MGPU_ENS_UPDATE_MINB) k_ens_update(const 
       const long long t = base + s;
       if (t < d.g.ninterior)
         update_zone<T, ND>(d.g, a, U0, U1, (const T *) d.b.F[0], (const T *) d.b.F[1], (const T *) d.b.F[2], Uout,
-                       Kout, K1, K2, K3, dt, t);
+                           Kout, K1, K2, K3, dt, interior_zone(d.g, t));
     }
   }
 }

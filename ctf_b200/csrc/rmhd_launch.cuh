@@ -110,11 +110,16 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
     const StateCPtr<T> cU0{U0.bulk, U0.B}, cU1{U1.bulk, U1.B}, cK0{K[0].bulk, K[0].B}, cK1{K[1].bulk, K[1].B},
         cK2{K[2].bulk, K[2].B};
+    const int march = MGPU_UPDATE_MARCH;
     if (g.nd == 1)
       k_update<T, 1><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
     else if (g.nd == 2)
       k_update<T, 2><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
-    else
+    else if (march > 0) {
+      const long long threads = (long long) g.n[1] * g.n[2] * ((g.n[0] + march - 1) / march);
+      k_update_march<T, 3><<<(unsigned) ((threads + zb - 1) / zb), zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout,
+                                                                                cK0, cK1, cK2, A.ctl, s, march);
+    } else
       k_update<T, 3><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
   } else if (phase == PH_COMMIT) {
     ProfScope ps(pr, st, KC_BEGIN, 1);

@@ -72,11 +72,12 @@ def test_uneven_kh_boxes_match_single_solvers_fp64():
         assert np.array_equal(got[b], ref[b]), (b, np.abs(got[b] - ref[b]).max())
 
 
-@pytest.mark.parametrize("steps,tol", [(1, 1e-6), (6, 1e-5)])
+@pytest.mark.parametrize("steps,tol", [(1, 1e-6), (6, 1e-3)])
 def test_uneven_kh_boxes_track_single_solvers_fp32(steps, tol):
     """FP32-bulk kernels of the ensemble and of the single-box path are compiled separately
-    with FMA contraction on, so they may round differently; they agree to FP32 accuracy
-    (the bound of the FP32-vs-FP64 comparison)."""
+    with FMA contraction on, so they may round differently: after one step they agree to
+    1e-6; over six steps HLLC's division by the (small, growing) normal field on y faces
+    amplifies those roundings to ~2e-4 in places (the HLLC bound of test_gpu_fp32.py)."""
     sizes = [(24, 20), (32, 32), (16, 40), (48, 24), (20, 20), (36, 28)]
     scheme = Scheme(extrap="plm", riemann="hllc", advance="rk3", precision="fp32")
     states = kh_states(sizes, seed=3)

@@ -10,6 +10,14 @@
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
 #endif
+// Two 128-zone tiles in flight per CTA of the tensor-core c2p (1), or one (0); the paired
+// kernel's 55 KB of shared memory allows 3 CTAs per SM.
+#ifndef MGPU_TC_PAIRS
+#define MGPU_TC_PAIRS 1
+#endif
+#ifndef MGPU_TC2_CTAS_PER_SM
+#define MGPU_TC2_CTAS_PER_SM 3
+#endif
 
 namespace mgpu {
 
@@ -78,7 +86,19 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
     const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
-    if (tc_c2p)
+    if (tc_c2p && MGPU_TC_PAIRS) {
+      static bool smem_set = false;   // 55 KB of dynamic shared memory needs the opt-in
+      if (!smem_set) {
+        const cudaError_t e = cudaFuncSetAttribute(k_cons_to_prim_tc2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   tc::SMEM2_BYTES);
+        if (e != cudaSuccess) return e;
+        smem_set = true;
+      }
+      const long long npairs = (g.ninterior + 255) / 256;
+      const long long pmax = 148ll * MGPU_TC2_CTAS_PER_SM;
+      k_cons_to_prim_tc2<T><<<(unsigned) (npairs < pmax ? npairs : pmax), 128, tc::SMEM2_BYTES, st>>>(
+          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
+    } else if (tc_c2p)
       k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
                                                                 final, A.ereset, A.preset, A.dreset);
     else if (simt_net)
@@ -110,16 +130,11 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
     const StateCPtr<T> cU0{U0.bulk, U0.B}, cU1{U1.bulk, U1.B}, cK0{K[0].bulk, K[0].B}, cK1{K[1].bulk, K[1].B},
         cK2{K[2].bulk, K[2].B};
-    const int march = MGPU_UPDATE_MARCH;
     if (g.nd == 1)
       k_update<T, 1><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
     else if (g.nd == 2)
       k_update<T, 2><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
-    else if (march > 0) {
-      const long long threads = (long long) g.n[1] * g.n[2] * ((g.n[0] + march - 1) / march);
-      k_update_march<T, 3><<<(unsigned) ((threads + zb - 1) / zb), zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout,
-                                                                                cK0, cK1, cK2, A.ctl, s, march);
-    } else
+    else
       k_update<T, 3><<<zgrid, zb, 0, st>>>(g, ua, cU0, cU1, F, G, H, Uout, Kout, cK0, cK1, cK2, A.ctl, s);
   } else if (phase == PH_COMMIT) {
     ProfScope ps(pr, st, KC_BEGIN, 1);

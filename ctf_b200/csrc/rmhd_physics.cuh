@@ -813,46 +813,6 @@ __device__ __forceinline__ int riemann_hllc(T gamma, const T *pl, const T *pr, T
   return 0;
 }
 
-// The part of a Riemann solve that MaxLambda sees: each solver's own face states (HLLD: the
-// normal-frame permutation with the averaged normal field; HLLC: the averaged normal field;
-// HLL: as given), their P->U and fast speeds, and the max |lambda| update -- the same
-// arithmetic, in the same order, as the full solvers before their first use of the speeds.
-// Returns 1 where the full solver would (a side state with no conserved counterpart).
-template <class T, int dim, int RS>
-__device__ __forceinline__ int riemann_speeds(const PhysParams &pp, const T *pl, const T *pr, T &ml)
-{
-  using M = DimMap<dim>;
-  constexpr int B1 = M::B1;
-  const T gamma = T(pp.gamma);
-  T Pl[8], Pr[8], Ul[8], Ur[8], Fs[8], epl, eml, epr, emr;
-  int fdim = dim;
-  if constexpr (RS == RIEMANN_HLLD) {
-    constexpr int B2 = M::B2, B3 = M::B3, v1 = M::v1, v2 = M::v2, v3 = M::v3;
-    Pl[pre] = pl[pre]; Pr[pre] = pr[pre];
-    Pl[rho] = pl[rho]; Pr[rho] = pr[rho];
-    Pl[vx] = pl[v1];   Pr[vx] = pr[v1];
-    Pl[vy] = pl[v2];   Pr[vy] = pr[v2];
-    Pl[vz] = pl[v3];   Pr[vz] = pr[v3];
-    Pl[By] = pl[B2];   Pr[By] = pr[B2];
-    Pl[Bz] = pl[B3];   Pr[Bz] = pr[B3];
-    Pl[Bx] = Pr[Bx] = T(0.5) * (pl[B1] + pr[B1]);
-    fdim = 1;
-  } else {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) { Pl[i] = pl[i]; Pr[i] = pr[i]; }
-    if constexpr (RS == RIEMANN_HLLC) Pl[B1] = Pr[B1] = T(0.5) * (Pl[B1] + Pr[B1]);
-  }
-  if (prim_to_cons(gamma, Pl, Ul)) return 1;
-  if (prim_to_cons(gamma, Pr, Ur)) return 1;
-  flux_and_eigenvalues(gamma, Ul, Pl, Fs, epl, eml, fdim);
-  flux_and_eigenvalues(gamma, Ur, Pr, Fs, epr, emr, fdim);
-  const T ap = (epl > epr) ? epl : epr;
-  const T am = (eml < emr) ? eml : emr;
-  const T l = face_lambda(ap, am);
-  if (ml < l) ml = l;
-  return 0;
-}
-
 // Out-of-line HLLC for the HLLD fallback (rare): arguments and result by value so that the
 // caller's face states stay in registers on its hot path.
 template <class T> struct Face8 { T v[8]; };

@@ -228,24 +228,6 @@ struct FluxTally {
 
 // One face: reconstruct, Riemann solve (PCM retry on failure), store the flux; the face's
 // |lambda| is folded into ml.
-// Whether some interior zone's update reads the dim-sweep flux stored at zone f: the
-// divergence reads faces f and f - S of interior zones, the corner EMFs those of their
-// transverse neighbours, so the face's own coordinate along the sweep must lie in
-// [ng - 1, G - ng - 1] and its transverse coordinates in [ng - 1, G - ng].
-template <int dim>
-__device__ __forceinline__ bool face_needed(const Grid &g, long long f)
-{
-  const int c[3] = {(int) (f / g.s[0]), (int) ((f / g.s[1]) % g.G[1]), (int) (f % g.G[2])};
-  const int lo = g.ng - 1;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (d >= g.nd) continue;
-    const int hi = (d == dim - 1) ? g.G[d] - g.ng - 1 : g.G[d] - g.ng;
-    if (c[d] < lo || c[d] > hi) return false;
-  }
-  return true;
-}
-
 template <class T, int dim, int RS>
 __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ PA, T *__restrict__ F,
                                           const PhysParams &pp, long long f, T &ml, FluxTally &ft)
@@ -273,26 +255,6 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
   const T gamma = T(pp.gamma);
   int err = 1, used_hllc = 0;
   constexpr bool hlld = RS == RIEMANN_HLLD;
-  // Faces that no interior update reads (those more than one guard layer out across the
-  // sweep, or more than one layer into the guards along it -- including the faces whose
-  // stencils wrap across a row of the flattened array) still enter MaxLambda: for them only
-  // the speeds are computed, with the full solver's arithmetic and PCM retry, and a zero
-  // flux is stored.
-  if (!face_needed<dim>(g, f)) {
-    int e = riemann_speeds<T, dim, RS>(pp, Pl, Pr, ml);
-    if (e) {
-      ft.pcm_retry += 1;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        Pl[q] = PA[q * g.cs + f];
-        Pr[q] = PA[q * g.cs + f + S];
-      }
-      riemann_speeds<T, dim, RS>(pp, Pl, Pr, ml);
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) F[q * g.cs + f] = T(0);
-    return;
-  }
   C2PTally tally{0, 0};
   // attempt 0: reconstructed states; attempt 1: the zone states themselves (PCM retry).
   // One call site per solver keeps a single inlined copy of it.
@@ -490,9 +452,7 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
 #ifndef MGPU_UPDATE_MINB
 #define MGPU_UPDATE_MINB 4   // 64 registers: chosen by a sweep of 3-4 (the natural count, 74, allows 3)
 #endif
-#ifndef MGPU_UPDATE_MARCH
-#define MGPU_UPDATE_MARCH 16  // x-chunk length of the marching update (0: one zone per thread)
-#endif
+
 template <class T, int ND>
 __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_update(Grid g, UpdateArgs a, StateCPtr<T> Un, StateCPtr<T> Us,
                                                 const T *__restrict__ F, const T *__restrict__ G,
@@ -504,35 +464,6 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_update(Grid g, Update
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.ninterior) return;
   update_zone<T, ND>(g, a, Un, Us, F, G, H, Uout, Kout, K1, K2, K3, ctl->dt, interior_zone(g, t));
-}
-
-// The same update, each thread marching along x through a chunk of `len` zones of one
-// (j, k) column: the x-neighbour planes of the divergence and the corner EMFs were read by
-// the same thread one step earlier (L1), instead of by blocks a whole plane away, whose
-// planes outgrow the L2 on large boxes (a 518^2 plane of one FP32 component is 1 MB and the
-// update touches ~30 arrays).  Threads: k fastest, then j, then the x chunk.
-template <class T, int ND>
-__global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_update_march(Grid g, UpdateArgs a, StateCPtr<T> Un,
-                                                                        StateCPtr<T> Us, const T *__restrict__ F,
-                                                                        const T *__restrict__ G,
-                                                                        const T *__restrict__ H, StatePtr<T> Uout,
-                                                                        StatePtr<T> Kout, StateCPtr<T> K1,
-                                                                        StateCPtr<T> K2, StateCPtr<T> K3,
-                                                                        const Ctl *ctl, int stage, int len)
-{
-  if (stage_failed(ctl, stage + 1)) return;
-  const long long cols = (long long) g.n[1] * g.n[2];
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  const long long chunk = t / cols;
-  if (chunk * len >= g.n[0]) return;
-  const long long c = t - chunk * cols;
-  const int j = (int) (c / g.n[2]) + (g.nd >= 2 ? g.ng : 0);
-  const int k = (int) (c % g.n[2]) + (g.nd >= 3 ? g.ng : 0);
-  const int i0 = g.ng + (int) (chunk * len);
-  const int i1 = min(i0 + len, g.ng + g.n[0]);
-  const double dt = ctl->dt;
-  for (int i = i0; i < i1; ++i)
-    update_zone<T, ND>(g, a, Un, Us, F, G, H, Uout, Kout, K1, K2, K3, dt, ((long long) i * g.G[1] + j) * g.G[2] + k);
 }
 
 }  // namespace mgpu

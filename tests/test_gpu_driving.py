@@ -10,7 +10,7 @@ from ctf_b200.mara import Scheme, Solver, new_ou_field
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 5e-5)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 5e-3)])   # FP32: the L-inf bound of test_gpu_fp32
 def test_driven_box_matches_the_reference(precision, tol):
     from oracle import RefOracle, Scheme as OScheme
     n = (12, 12, 12)

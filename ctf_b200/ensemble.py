@@ -199,9 +199,9 @@ class Ensemble:
         return db[key]
 
 
-def kh_sizes(nboxes: int = 256, seed: int = 0, lo: int = 64, hi: int = 512):
-    """Box sizes log-uniform in lo^2..hi^2 (square boxes, sides rounded to even)."""
+def kh_sizes(nboxes: int = 256, seed: int = 0, lo: int = 64, hi: int = 512, multiple: int = 8):
+    """Box sizes log-uniform in lo^2..hi^2 (square boxes, sides rounded to a multiple of 8)."""
     rng = np.random.default_rng(seed)
     sides = np.exp(rng.uniform(np.log(lo), np.log(hi), nboxes))
-    sides = (np.round(sides / 2) * 2).astype(int)
+    sides = np.clip(np.round(sides / multiple) * multiple, multiple, None).astype(int)
     return [(int(n), int(n)) for n in sides]

@@ -30,6 +30,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
 RECON = {"pcm": 0, "plm": 1, "weno5": 2}
+GODUNOV = {"plm-split": 0, "plm-muscl": 1}
 RIEMANN = {"hll": 0, "hllc": 1, "hlld": 2}
 ADVANCE = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}
 IS_MODE = {"js96": 0, "b08": 1, "sz10": 2}
@@ -53,6 +54,7 @@ class Scheme:
     ereset: bool = False
     preset: float = 1.0
     dreset: float = 1.0
+    godunov: str = "plm-split"
 
     @property
     def nd(self) -> int:
@@ -79,7 +81,7 @@ class _PortConfig(ctypes.Structure):
                 ("theta", ctypes.c_double), ("is_mode", ctypes.c_int),
                 ("sz10A", ctypes.c_double), ("riemann", ctypes.c_int), ("rk", ctypes.c_int),
                 ("pfloor", ctypes.c_double), ("ereset", ctypes.c_int),
-                ("preset", ctypes.c_double), ("dreset", ctypes.c_double)]
+                ("preset", ctypes.c_double), ("dreset", ctypes.c_double), ("godunov", ctypes.c_int)]
 
 
 class _PortStats(ctypes.Structure):
@@ -115,6 +117,7 @@ class PortOracle:
         c.ereset = int(scheme.ereset)
         c.preset = scheme.preset
         c.dreset = scheme.dreset
+        c.godunov = GODUNOV[scheme.godunov]
         self.cfg = c
         self.stats = _PortStats()
         L = self.lib
@@ -214,7 +217,7 @@ class RefOracle:
         L.ref_open()
         lua = (f"Mara.start(); Mara.set_fluid('rmhd'); Mara.set_eos('gamma-law', {s.gamma!r}); "
                f"Mara.set_boundary('periodic'); Mara.set_riemann('{s.riemann}'); "
-               f"Mara.set_godunov('plm-split'); Mara.set_advance('{s.advance}'); "
+               f"Mara.set_godunov('{s.godunov}'); Mara.set_advance('{s.advance}'); "
                f"Mara.config_solver({{extrap='{s.extrap}', theta={s.theta!r}, IS='{s.IS}', "
                f"sz10A={s.sz10A!r}, pfloor={s.pfloor!r}, ereset={'true' if s.ereset else 'false'}, "
                f"preset={s.preset!r}, dreset={s.dreset!r}}}, true); "

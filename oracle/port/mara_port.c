@@ -1110,8 +1110,8 @@ static void flux_sweep(const port_config *c, port_stats *st, const grid_t *g,
 
 /* MethodOfLinesSplit::dUdt + drive_sweeps_{1,2,3}d (Mara/plm-split.cpp:11-122).
  * Returns the c2p failure count (non-zero aborts the step); L is the time derivative. */
-static int dUdt(const port_config *c, port_stats *st, const grid_t *g, const double *Uin,
-                double *PA, double *L)
+static int dUdt_split(const port_config *c, port_stats *st, const grid_t *g, const double *Uin,
+                      double *PA, double *L)
 {
   const long n = g->nz * 8;
   double *U = malloc(n * sizeof(double));
@@ -1144,6 +1144,144 @@ static int dUdt(const port_config *c, port_stats *st, const grid_t *g, const dou
   return 0;
 }
 
+/* ---- PlmCtuHancockOperator (Mara/ctu-hancock.cpp:53-494), default safety level ---------- */
+/* its own minmod, with the static plm_theta that config_solver{theta} sets (:27-35) */
+static double ctu_minmod(double theta, double ul, double u0, double ur)
+{
+  const double a = theta * (u0 - ul);
+  const double b = 0.5 * (ur - ul);
+  const double cc = theta * (ur - u0);
+  const double sa = SGN(a), sb = SGN(b), sc = SGN(cc);
+  const double fa = fabs(a), fb = fabs(b), fc = fabs(cc);
+  const double ab = (fa < fb) ? fa : fb;
+  const double m = (ab < fc) ? ab : fc;
+  return 0.25 * fabs(sa + sb) * (sa + sc) * m;
+}
+
+/* dUdt of the CTU-Hancock operator: c2p of U into PA, slopes, first (transverse) fluxes,
+ * per-direction Hancock predictors with their c2p, final fluxes from the predicted states,
+ * CT and the divergence.  Returns the failure count of the first check that fails (each
+ * aborts the step, :215, :334, :375, :494); L is the time derivative. */
+static int dUdt_ctu(const port_config *c, port_stats *st, const grid_t *g, const double *Uin,
+                    double *PA, double *L, double dt)
+{
+  const long n = g->nz * 8;
+  const int nd = c->nd;
+  const long S0 = g->stride[0];
+  const long sx = g->stride[1], sy = g->stride[2], sz = g->stride[3];
+  const long Sd[3] = {sx, sy, sz};
+  double *U = malloc(n * sizeof(double));
+  memcpy(U, Uin, n * sizeof(double));
+  /* the c2p count is not checked here (:61-66): failed zones keep what the inversion left in
+   * PA, and ctu_hancock clears FailureMask before its own checks (:102) */
+  c2p_all(c, g, U, PA);
+  int fail = 0;
+  const double *P = PA;
+  double *Fd[3] = {NULL, NULL, NULL}, *dP[3] = {NULL, NULL, NULL}, *Ud[3] = {NULL, NULL, NULL};
+  double *Pd[3] = {NULL, NULL, NULL};
+  for (int d = 0; d < nd; ++d) {
+    Fd[d] = calloc(n, sizeof(double));
+    dP[d] = calloc(n, sizeof(double));
+    Ud[d] = calloc(n, sizeof(double));
+    Pd[d] = calloc(n, sizeof(double));
+  }
+  double Pl[8], Pr[8];
+  /* step 1: slopes */
+  for (long i = sx; i < S0 - sx; ++i)
+    for (int d = 0; d < nd; ++d) dP[d][i] = ctu_minmod(c->theta, P[i - Sd[d]], P[i], P[i + Sd[d]]);
+  /* step 2: fluxes of the reconstructed zone-centre states, every direction */
+  for (long i = 0; i < S0 - sx; i += 8)
+    for (int d = 0; d < nd; ++d) {
+      for (int j = 0; j < 8; ++j) {
+        Pr[j] = P[i + Sd[d] + j] - 0.5 * dP[d][i + Sd[d] + j];
+        Pl[j] = P[i + j] + 0.5 * dP[d][i + j];
+      }
+      if (check_prim(Pl) || check_prim(Pr)) fail += 1;
+      else port_riemann(c, st, Pl, Pr, &Fd[d][i], d + 1);
+    }
+  if (fail) goto done;
+  /* step 3: Hancock predictors, normal flux difference of the zone's own face states plus the
+   * transverse Godunov fluxes, half a step */
+  for (long i = sx; i < S0; i += 8) {
+    double FL[3][8], FR[3][8], UL[8], UR[8], PL[8], PR[8];
+    for (int d = 0; d < nd; ++d) {
+      for (int j = 0; j < 8; ++j) {
+        PL[j] = P[i + j] - 0.5 * dP[d][i + j];
+        PR[j] = P[i + j] + 0.5 * dP[d][i + j];
+      }
+      if (check_prim(PL) || check_prim(PR)) {
+        fail += 1;
+        memset(FL[d], 0, sizeof(FL[d]));
+        memset(FR[d], 0, sizeof(FR[d]));
+      } else {
+        port_prim_to_cons(c, PL, UL);
+        port_prim_to_cons(c, PR, UR);
+        port_flux_and_eigenvalues(c, UL, PL, FL[d], NULL, NULL, d + 1);   /* no speeds (:262) */
+        port_flux_and_eigenvalues(c, UR, PR, FR[d], NULL, NULL, d + 1);
+      }
+    }
+    for (int j = 0; j < 8; ++j) {
+      const long m = i + j;
+      if (nd == 1) {
+        Ud[0][m] = U[m] - ((FR[0][j] - FL[0][j]) / g->dx) * 0.5 * dt;
+      } else if (nd == 2) {
+        Ud[0][m] = U[m] - ((FR[0][j] - FL[0][j]) / g->dx + (Fd[1][m] - Fd[1][m - sy]) / g->dy) * 0.5 * dt;
+        Ud[1][m] = U[m] - ((FR[1][j] - FL[1][j]) / g->dy + (Fd[0][m] - Fd[0][m - sx]) / g->dx) * 0.5 * dt;
+      } else {
+        Ud[0][m] = U[m] - ((FR[0][j] - FL[0][j]) / g->dx + (Fd[1][m] - Fd[1][m - sy]) / g->dy +
+                           (Fd[2][m] - Fd[2][m - sz]) / g->dz) * 0.5 * dt;
+        Ud[1][m] = U[m] - ((FR[1][j] - FL[1][j]) / g->dy + (Fd[2][m] - Fd[2][m - sz]) / g->dz +
+                           (Fd[0][m] - Fd[0][m - sx]) / g->dx) * 0.5 * dt;
+        Ud[2][m] = U[m] - ((FR[2][j] - FL[2][j]) / g->dz + (Fd[0][m] - Fd[0][m - sx]) / g->dx +
+                           (Fd[1][m] - Fd[1][m - sy]) / g->dy) * 0.5 * dt;
+      }
+    }
+  }
+  if (fail) goto done;
+  /* predicted primitives: guards from the periodic fill, c2p from the zone's primitives */
+  for (int d = 0; d < nd; ++d) sync_periodic(c, g, Ud[d]);
+  for (long i = 0; i < S0; i += 8)
+    for (int d = 0; d < nd; ++d) {
+      memcpy(&Pd[d][i], &P[i], 8 * sizeof(double));
+      if (port_cons_to_prim(c, &Ud[d][i], &Pd[d][i])) fail += 1;
+    }
+  if (fail) goto done;
+  /* step 4: fluxes of the predicted states (a face keeps its step-2 flux where the solver
+   * fails) */
+  for (long i = sx; i < S0 - sx; i += 8)
+    for (int d = 0; d < nd; ++d) {
+      for (int j = 0; j < 8; ++j) {
+        Pr[j] = Pd[d][i + Sd[d] + j] - 0.5 * dP[d][i + Sd[d] + j];
+        Pl[j] = Pd[d][i + j] + 0.5 * dP[d][i + j];
+      }
+      if (check_prim(Pl) || check_prim(Pr)) fail += 1;
+      else port_riemann(c, st, Pl, Pr, &Fd[d][i], d + 1);
+    }
+  memset(L, 0, n * sizeof(double));
+  if (nd == 1) {
+    for (long i = sx; i < S0; ++i) L[i] = -((Fd[0][i] - Fd[0][i - sx]) / g->dx);
+  } else if (nd == 2) {
+    port_ct2d(Fd[0], Fd[1], g->stride);
+    for (long i = sx; i < S0; ++i) L[i] = -((Fd[0][i] - Fd[0][i - sx]) / g->dx + (Fd[1][i] - Fd[1][i - sy]) / g->dy);
+  } else {
+    port_ct3d(Fd[0], Fd[1], Fd[2], g->stride);
+    for (long i = sx; i < S0; ++i)
+      L[i] = -((Fd[0][i] - Fd[0][i - sx]) / g->dx + (Fd[1][i] - Fd[1][i - sy]) / g->dy +
+               (Fd[2][i] - Fd[2][i - sz]) / g->dz);
+  }
+done:
+  for (int d = 0; d < nd; ++d) { free(Fd[d]); free(dP[d]); free(Ud[d]); free(Pd[d]); }
+  free(U);
+  return fail;
+}
+
+/* GodunovOperator::dUdt of the selected operator (set_godunov, Mara/mara.cpp:960-994) */
+static int dUdt(const port_config *c, port_stats *st, const grid_t *g, const double *Uin, double *PA,
+                double *L, double dt)
+{
+  return c->godunov ? dUdt_ctu(c, st, g, Uin, PA, L, dt) : dUdt_split(c, st, g, Uin, PA, L);
+}
+
 /* luaC_Mara_advance (Mara/mara.cpp:297-341) with the Runge-Kutta integrators of
  * Mara/runge-kutta.hpp:129-177.  prim is updated only when no zone fails. */
 int port_advance(const port_config *c, port_stats *st, double *prim, double dt, int *errors)
@@ -1163,33 +1301,33 @@ int port_advance(const port_config *c, port_stats *st, double *prim, double dt, 
   long i;
   switch (c->rk) {
   case 1:
-    if ((err = dUdt(c, st, &g, U, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U[i] += dt * L[i];
     break;
   case 2:
-    if ((err = dUdt(c, st, &g, U, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U1[i] = U[i] + dt * L[i];
-    if ((err = dUdt(c, st, &g, U1, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U1, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U[i] = 0.5 * (U[i] + U1[i] + dt * L[i]);
     break;
   case 3:
-    if ((err = dUdt(c, st, &g, U, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U1[i] = U[i] + dt * L[i];
-    if ((err = dUdt(c, st, &g, U1, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U1, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U1[i] = 3. / 4 * U[i] + 1. / 4 * U1[i] + 1. / 4 * dt * L[i];
-    if ((err = dUdt(c, st, &g, U1, PA, L))) break;
+    if ((err = dUdt(c, st, &g, U1, PA, L, dt))) break;
     for (i = 0; i < n; ++i) U[i] = 1. / 3 * U[i] + 2. / 3 * U1[i] + 2. / 3 * dt * L[i];
     break;
   default: {
     double *L1 = malloc(n * sizeof(double)), *L2 = malloc(n * sizeof(double));
     double *L3 = malloc(n * sizeof(double));
-    if (!(err = dUdt(c, st, &g, U, PA, L))) {
+    if (!(err = dUdt(c, st, &g, U, PA, L, dt))) {
       for (i = 0; i < n; ++i) { L1[i] = dt * L[i]; U1[i] = U[i] + 0.5 * L1[i]; }
-      if (!(err = dUdt(c, st, &g, U1, PA, L))) {
+      if (!(err = dUdt(c, st, &g, U1, PA, L, dt))) {
         for (i = 0; i < n; ++i) { L2[i] = dt * L[i]; U1[i] = U[i] + 0.5 * L2[i]; }
-        if (!(err = dUdt(c, st, &g, U1, PA, L))) {
+        if (!(err = dUdt(c, st, &g, U1, PA, L, dt))) {
           for (i = 0; i < n; ++i) { L3[i] = dt * L[i]; U1[i] = U[i] + 1.0 * L3[i]; }
-          if (!(err = dUdt(c, st, &g, U1, PA, L))) {
+          if (!(err = dUdt(c, st, &g, U1, PA, L, dt))) {
             for (i = 0; i < n; ++i)
               U[i] += (1.0 / 6.0) * (L1[i] + 2.0 * L2[i] + 2.0 * L3[i] + dt * L[i]);
           }

@@ -29,6 +29,7 @@ typedef struct {
   double pfloor;      /* c2p pressure floor, disabled when <= 0 */
   int    ereset;      /* emergency reset of failed zones */
   double preset, dreset;
+  int    godunov;     /* 0 plm-split (MethodOfLinesSplit), 1 plm-muscl (PlmCtuHancockOperator) */
 } port_config;
 
 typedef struct {

@@ -4,7 +4,7 @@ Runs only where the reference sources are available (``make -C oracle ref`` buil
 ``oracle/_ref/libmara_ref.so`` from them); the fixtures it writes are committed so that the
 tests need neither the reference nor its build on any other machine.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]     # all fixtures, or the named step cases
 
 Fixtures (all float64, AoS primitive layout with 3 guard zones where a grid is involved):
   step_*.npz      whole-step runs through Mara.advance / Mara.get_timestep
@@ -44,7 +44,26 @@ STEP_CASES = {
                                  advance="rk2"), lambda: ics.kh_box((16, 12), seed=16), 4, 0.3),
     "hllc_fail_12": (dict(n=(12, 12, 12), riemann="hllc", advance="rk3"),
                     lambda: ics.turbulence_box((12, 12, 12), seed=1), 3, 0.3),
+    # CTU-Hancock (set_godunov('plm-muscl')): the healthy step of ctf-core/drvtrb.lua:296-302
+    # (single, HLLD, theta 2, CFL 0.24) and its fallbacks, in 3D, 2D and 1D
+    "ctu_plm_hlld_single_8": (dict(n=(8, 8, 8), godunov="plm-muscl", advance="single"),
+                              lambda: ics.turbulence_box((8, 8, 8), seed=17), 6, 0.24),
+    "ctu_hll_rk2_odd": (dict(n=(9, 7, 6), godunov="plm-muscl", riemann="hll", advance="rk2",
+                             theta=1.25), lambda: ics.turbulence_box((9, 7, 6), seed=18), 4, 0.3),
+    "ctu_kh2d_hllc_rk3": (dict(n=(16, 12), x0=(0.0, 0.0), x1=(1.0, 1.0), godunov="plm-muscl",
+                               riemann="hllc", advance="rk3", theta=1.5),
+                          lambda: ics.kh_box((16, 12), seed=19), 4, 0.3),
+    "ctu_1d_hlld_single": (dict(n=(24,), x0=(0.0,), x1=(1.0,), godunov="plm-muscl",
+                                advance="single"), lambda: _line((24,), seed=20), 6, 0.3),
+    "ctu_fail_8": (dict(n=(8, 7, 6), godunov="plm-muscl", riemann="hllc", advance="rk2"),
+                   lambda: ics.turbulence_box((8, 7, 6), seed=1, vrms=0.4), 6, 0.4),
 }
+
+
+def _line(n, seed):
+    """A 1D box: the x line through a 3D turbulence box, guards included."""
+    P = ics.turbulence_box((n[0], 4, 4), seed=seed, vrms=0.5)
+    return np.ascontiguousarray(P[:, 3, 3].reshape(n[0] + 6, 1, 1, 8))
 
 
 def step_fixture(name, kw, ic, steps, cfl):
@@ -159,8 +178,11 @@ def function_fixtures():
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]          # fixture names to (re)generate; none: all of them
     for name, (kw, ic, steps, cfl) in STEP_CASES.items():
-        step_fixture(name, kw, ic, steps, cfl)
-    function_fixtures()
+        if not only or name in only:
+            step_fixture(name, kw, ic, steps, cfl)
+    if not only or "functions" in only:
+        function_fixtures()
     total = sum(os.path.getsize(os.path.join(OUT, f)) for f in os.listdir(OUT) if f.endswith(".npz"))
     print(f"wrote {total / 1e6:.2f} MB of fixtures")

@@ -83,7 +83,7 @@ def test_ensemble_box_sizes_are_log_uniform():
     sizes = kh_sizes(256, seed=0)
     sides = np.array([s[0] for s in sizes])
     assert len(sizes) == 256 and all(s[0] == s[1] for s in sizes)
-    assert sides.min() >= 64 and sides.max() <= 512 and np.all(sides % 2 == 0)
+    assert sides.min() >= 64 and sides.max() <= 512 and np.all(sides % 8 == 0)
     # log-uniform: the median side is near the geometric mean sqrt(64 * 512) = 181
     assert 150 <= np.median(sides) <= 215
     assert kh_sizes(256, seed=0) == sizes

@@ -23,7 +23,7 @@ class MgpuConfig(ctypes.Structure):
                 ("theta", ctypes.c_double), ("is_mode", ctypes.c_int), ("sz10A", ctypes.c_double),
                 ("riemann", ctypes.c_int), ("rk", ctypes.c_int), ("pfloor", ctypes.c_double),
                 ("ereset", ctypes.c_int), ("preset", ctypes.c_double), ("dreset", ctypes.c_double),
-                ("precision", ctypes.c_int), ("learned_c2p", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("learned_c2p", ctypes.c_int), ("godunov", ctypes.c_int)]
 
 
 class MgpuStats(ctypes.Structure):

@@ -218,6 +218,7 @@ int mgpu_default_config(mgpu_config *c)
   c->dreset = 1.0;
   c->precision = MGPU_PREC_FP64;
   c->learned_c2p = 0;
+  c->godunov = MGPU_GODUNOV_PLM_SPLIT;
   return MGPU_OK;
 }
 
@@ -231,6 +232,8 @@ static int check_config(mgpu_solver *h, const mgpu_config *c)
   if (c->is_mode < 0 || c->is_mode > 2) return fail(h, MGPU_ERR_ARG, "no such IS");
   if (c->precision != MGPU_PREC_FP64 && c->precision != MGPU_PREC_FP32)
     return fail(h, MGPU_ERR_ARG, "no such precision");
+  if (c->godunov != MGPU_GODUNOV_PLM_SPLIT && c->godunov != MGPU_GODUNOV_PLM_MUSCL)
+    return fail(h, MGPU_ERR_ARG, "no such integration scheme");
   return MGPU_OK;
 }
 
@@ -363,6 +366,11 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
     if (d < nd) e = dalloc(h, &h->b.F[d], 8 * cs * tsz);
     else h->b.F[d] = h->b.F[0];
   }
+  // CTU-Hancock: predicted primitives of each direction
+  for (int d = 0; d < 3 && e == cudaSuccess && h->cfg.godunov == MGPU_GODUNOV_PLM_MUSCL; ++d) {
+    if (d < nd) e = dalloc(h, &h->b.Pd[d], 8 * cs * tsz);
+    else h->b.Pd[d] = h->b.Pd[0];
+  }
   h->staging_zones = g.nz < (1ll << 22) ? g.nz : (1ll << 22);   // up to 256 MB of AoS
   if (e == cudaSuccess) e = dalloc(h, (void **) &h->staging, (size_t) h->staging_zones * 8 * sizeof(double));
   if (e == cudaSuccess) e = dalloc(h, (void **) &h->red, sizeof(double) * 2 * RED_BLOCKS);
@@ -458,6 +466,7 @@ static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
   A.g = h->g;
   A.pp = phys(h);
   A.rk = h->cfg.rk;
+  A.godunov = h->cfg.godunov;
   A.ereset = h->cfg.ereset;
   A.preset = h->cfg.preset;
   A.dreset = h->cfg.dreset;
@@ -703,6 +712,7 @@ int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double
   A.g = h->g;
   A.pp = phys(h);
   A.rk = h->cfg.rk;
+  A.godunov = h->cfg.godunov;
   A.ereset = h->cfg.ereset;
   A.preset = h->cfg.preset;
   A.dreset = h->cfg.dreset;
@@ -739,6 +749,8 @@ int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult)
   for (int d = 0; d < g.nd; ++d)
     if (ext[d]) total += g.n[d];
   if (total > 0 && !mult) return fail(h, MGPU_ERR_ARG, "external guards need multiplicity tables");
+  if (total > 0 && h->cfg.godunov != MGPU_GODUNOV_PLM_SPLIT)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the CTU-Hancock operator runs on single domains only");
   for (long long i = 0; i < total; ++i)
     if (mult[i] < 1) return fail(h, MGPU_ERR_ARG, "multiplicities must be >= 1");
   if (h->mult) cudaFree(h->mult);

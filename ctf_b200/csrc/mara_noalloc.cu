@@ -68,9 +68,9 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   }
   if (cfg->fluid != MGPU_FLUID_RMHD || cfg->precision != MGPU_PREC_FP64 || cfg->rk < 1 || cfg->rk > 4 ||
       cfg->recon < 0 || cfg->recon > 2 || cfg->riemann < 0 || cfg->riemann > 2 || cfg->is_mode < 0 ||
-      cfg->is_mode > 2 || !(cfg->gamma > 1.0) || cfg->learned_c2p) {
+      cfg->is_mode > 2 || !(cfg->gamma > 1.0) || cfg->learned_c2p || cfg->godunov != MGPU_GODUNOV_PLM_SPLIT) {
     put_err(errbuf, errbuf_len,
-            "mgpu_advance_noalloc: needs an rmhd FP64 configuration without a learned c2p network");
+            "mgpu_advance_noalloc: needs an rmhd FP64 plm-split configuration without a learned c2p network");
     return MGPU_ERR_ARG;
   }
   if (nd < 1 || nd > 3) {
@@ -185,6 +185,7 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   A.pp.mlp = nullptr;
   A.pp.mlp_tc = nullptr;
   A.rk = cfg->rk;
+  A.godunov = 0;
   A.ereset = cfg->ereset;
   A.preset = cfg->preset;
   A.dreset = cfg->dreset;

@@ -1,11 +1,13 @@
 // Enqueues one advance (luaC_Mara_advance, Mara/mara.cpp:297-341) on a stream:
 //   begin (dt, reset MaxLambda) -> P->U -> per RK stage: c2p | flux x,y,z | CT+div+combine
 //   -> closing c2p into the uncommitted prim buffer -> commit if no zone failed.
+// With the CTU-Hancock operator a stage is c2p | CTU passes (rmhd_ctu.cuh) | CT+div+combine.
 // Nothing is read back: the host learns the outcome from the control block when it asks.
 #pragma once
 #include <algorithm>
 #include "rmhd_step.cuh"
 #include "rmhd_step_tc.cuh"
+#include "rmhd_ctu.cuh"
 
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
@@ -75,8 +77,9 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
   } else if (phase == PH_C2P) {
     // stage s < ns reads the stage input (U0 first, U1 after) into PA; s == ns is the
     // closing c2p of U0 into the uncommitted primitive buffer
-    const int final = s == ns;
-    const StateCPtr<T> Uin = (s == 0 || final) ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B};
+    // final: 1 closing c2p, 2 CTU-Hancock stage c2p (failures do not abort), 0 stage c2p
+    const int final = s == ns ? 1 : A.godunov ? 2 : 0;
+    const StateCPtr<T> Uin = (s == 0 || final == 1) ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B};
     const int zero_guess = s == 0;
     // learned guess on the tensor cores: persistent c2p kernel, MGPU_TC_CTAS_PER_SM CTAs per SM
     // (4 x 128 threads x 128 registers fill the register file)
@@ -108,7 +111,9 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
       k_cons_to_prim<T, 2><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
           g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
   } else if (phase == PH_FLUX_UPDATE) {
-    for (int d = 1; d <= g.nd; ++d) {
+    if (A.godunov)
+      launch_ctu_stage<T>(A, s, s == 0 ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B});
+    for (int d = 1; d <= g.nd && !A.godunov; ++d) {
       const long long S = g.s[d - 1];
       const long long nf = g.nz - 5 * S;
       if (nf <= 0) continue;

@@ -308,12 +308,13 @@ __device__ __forceinline__ void c2p_from_prim(const C2PState &s, const double *P
   W = sqrt(W2);
 }
 
-__device__ __forceinline__ int check_prim(const double *P)
+template <class T>
+__device__ __forceinline__ int check_prim(const T *P)
 {
-  const double v2 = P[vx] * P[vx] + P[vy] * P[vy] + P[vz] * P[vz];
-  if (v2 >= 1.0) return C2P_PRIM_SUPERLUMINAL;
-  if (P[pre] < 0.0) return C2P_PRIM_NEG_PRESSURE;
-  if (P[rho] < 0.0) return C2P_PRIM_NEG_RESTMASS;
+  const T v2 = P[vx] * P[vx] + P[vy] * P[vy] + P[vz] * P[vz];
+  if (v2 >= T(1)) return C2P_PRIM_SUPERLUMINAL;
+  if (P[pre] < T(0)) return C2P_PRIM_NEG_PRESSURE;
+  if (P[rho] < T(0)) return C2P_PRIM_NEG_RESTMASS;
 #pragma unroll
   for (int i = 0; i < 8; ++i)
     if (isnan(P[i])) return C2P_PRIM_NAN;

@@ -94,6 +94,8 @@ static __global__ void k_begin(Ctl *ctl, int dt_mode, double dt, double cfl, dou
     ctl->max_lambda_bits = 0ull;   // RiemannSolver::ResetMaxLambda
     for (int s = 0; s < MAX_STAGES; ++s) ctl->stage_err[s] = 0;
     ctl->final_err = 0;
+    for (int s = 0; s < 4; ++s) ctl->ctu_err[s] = 0;
+    ctl->ctu_c2p_err = ctl->ctu_reset = 0;
     ctl->committed = 0;
     ctl->c2p_calls = ctl->c2p_iters = 0;
     for (int a = 0; a < 6; ++a) ctl->c2p_attempt[a] = 0;
@@ -144,6 +146,10 @@ __global__ void __launch_bounds__(256) k_prim_to_cons(Grid g, StateCPtr<T> P0, S
 // Stage c2p (final == 0): guess from PA (or zeros on the first stage, as the reference's
 // PrimitiveArray is zero-filled by every advance, Mara/mara.cpp:321); result into PA.
 // Closing c2p (final == 1): guess from PA, result into the next committed state.
+// CTU-Hancock stage c2p (final == 2): as a stage c2p, but its failures do not abort the stage
+// (PlmCtuHancockOperator::dUdt ignores the count, Mara/ctu-hancock.cpp:61-66; a failed zone
+// keeps its guess) and its emergency resets are recorded, because the reset also replaces the
+// operator's conserved input by P->U of the repaired primitives (Mara/hydro.cpp:186-195).
 // Counts a zone's c2p outcome and scatters its primitives to the zone and its guard images.
 template <class T>
 __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn, Ctl *ctl, int stage, int final,
@@ -161,8 +167,10 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
       p[5] = u[5];
       p[6] = u[6];
       p[7] = u[7];
+      if (final == 2) atomicAdd(&ctl->ctu_reset, 1);
     } else {
-      atomicAdd(final ? &ctl->final_err : &ctl->stage_err[stage], multiplicity(g, i, j, k));
+      atomicAdd(final == 1 ? &ctl->final_err : final == 2 ? &ctl->ctu_c2p_err : &ctl->stage_err[stage],
+                multiplicity(g, i, j, k));
     }
   }
   int pi[3], pj[3], pk[3];
@@ -173,7 +181,7 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
     for (int b = 0; b < nj; ++b)
       for (int c = 0; c < nk; ++c) {
         const long long w = ((long long) pi[a] * g.G[1] + pj[b]) * g.G[2] + pk[c];
-        if (final) {
+        if (final == 1) {
 #pragma unroll
           for (int q = 0; q < 5; ++q) Pn.bulk[q * g.cs + w] = T(p[q]);
 #pragma unroll

@@ -44,6 +44,12 @@ struct Ctl {
   int cur;                              // committed primitive buffer (0/1)
   int committed;                        // 1 if the last advance was committed
   int tc_fault;                         // a tensor-core wait timed out (sticky)
+  // CTU-Hancock stage: failures of its four checks (first-flux face states, predictor face
+  // states, predictor c2p, second-flux face states), the uncounted stage c2p failures and the
+  // emergency resets of the stage c2p
+  int ctu_err[4];
+  int ctu_c2p_err;
+  int ctu_reset;
   // statistics, accumulated over the advance
   unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
   unsigned long long face_c2p_calls, face_c2p_iters;
@@ -94,11 +100,12 @@ struct AdvanceBuffers {
   void *U0_bulk, *U1_bulk, *K_bulk[3];
   double *U0_B, *U1_B, *K_B[3];
   void *F[3];
+  void *Pd[3];   // CTU-Hancock: predicted primitives per direction (8 x T each)
 };
 
 // Optional per-launch timing: the launcher records an event pair around every kernel and
 // tags it with its class (KC_*); the host sums the elapsed times after a synchronize.
-enum KernelClass { KC_BEGIN = 0, KC_P2C = 1, KC_C2P = 2, KC_FLUX = 3, KC_UPDATE = 4, KC_COUNT = 5 };
+enum KernelClass { KC_BEGIN = 0, KC_P2C = 1, KC_C2P = 2, KC_FLUX = 3, KC_UPDATE = 4, KC_PREDICT = 5, KC_COUNT = 6 };
 struct LaunchProfiler {
   cudaEvent_t *ev;    // 2 * capacity events
   int *tag;
@@ -131,6 +138,7 @@ struct AdvanceArgs {
   Grid g;
   PhysParams pp;
   int rk;           // 1 single, 2 rk2, 3 rk3, 4 rk4
+  int godunov;      // 0 method of lines (plm-split), 1 CTU-Hancock (plm-muscl)
   int ereset;
   double preset, dreset;
   int dt_mode;      // 0: dt from the host, 1: dt = cfl*min_dx/MaxLambda(previous)

@@ -133,9 +133,9 @@ class Ensemble:
 
     def profile_read(self) -> dict:
         """Per kernel class: summed ms, launches and work units since the last read."""
-        ms = (ctypes.c_double * 5)()
-        ln = (ctypes.c_longlong * 5)()
-        un = (ctypes.c_longlong * 5)()
+        ms = (ctypes.c_double * 6)()
+        ln = (ctypes.c_longlong * 6)()
+        un = (ctypes.c_longlong * 6)()
         self._check(self.lib.mgpu_ensemble_profile_read(self.h, ms, ln, un))
         return {k: {"ms": ms[i], "launches": ln[i], "units": un[i]}
                 for i, k in enumerate(Solver.KERNEL_CLASSES)}

@@ -5,7 +5,7 @@
  * runs the reference's driver loops unchanged for the RMHD step:
  *
  *   start, close, set_fluid('rmhd'), set_eos('gamma-law', G), set_boundary('periodic'),
- *   set_godunov('plm-split'), set_riemann, set_advance, config_solver{...}[, quiet],
+ *   set_godunov('plm-split' | 'plm-muscl'), set_riemann, set_advance, config_solver{...}[, quiet],
  *   set_domain(x0, x1, N, Nq, Ng), init_prim(buf, f), set_primitive(buf),
  *   advance(buf, dt) -> kzps, errors, get_timestep(CFL) -> dt,
  *   measure.mean_max_divB(), measure.max_lorentz_factor(), fluid.GetPrimNames()
@@ -47,9 +47,11 @@ typedef struct {
   long long net_count;
   char *drive;               /* driving field carried across a solver rebuild */
   long long drive_len;
+  int have_godunov;          /* set_godunov was called since start */
 } MaraGpu;
 
 static MaraGpu M;
+static double ctu_theta = 2.0;   /* the CTU-Hancock operator's plm_theta (a process static) */
 
 static void free_solver(void)
 {
@@ -79,7 +81,9 @@ static mgpu_solver *solver(lua_State *L)
     }
   }
   free_solver();
-  int rc = mgpu_create(&M.cfg, &M.h);
+  mgpu_config cfg = M.cfg;
+  if (cfg.godunov == MGPU_GODUNOV_PLM_MUSCL) cfg.theta = ctu_theta;
+  int rc = mgpu_create(&cfg, &M.h);
   if (rc) {
     M.h = NULL;
     luaL_error(L, "[Mara] could not create the GPU solver (code %d)", rc);
@@ -206,22 +210,28 @@ static int l_set_boundary(lua_State *L)
   return luaL_error(L, "[Mara] no such boundary conditions '%s'", key);
 }
 
-/* A new operator carries the constructor's emergency-reset settings (hydro.cpp:18-32). */
+/* A new operator carries the constructor's emergency-reset settings (hydro.cpp:18-32).
+ * 'plm-muscl' is the CTU-Hancock operator, whose PLM limiter parameter is its own
+ * process-wide static (ctu-hancock.cpp:11, default 2), changed only by config_solver{theta}
+ * while it is the current operator (mara.cpp:1068-1074). */
 static int l_set_godunov(lua_State *L)
 {
   const char *key = luaL_checkstring(L, 1);
-  if (strcmp(key, "plm-split") == 0) {
+  const int muscl = strcmp(key, "plm-muscl") == 0;
+  if (strcmp(key, "plm-split") == 0 || muscl) {
     mgpu_config d;
     mgpu_default_config(&d);
     M.cfg.ereset = d.ereset;
     M.cfg.preset = d.preset;
     M.cfg.dreset = d.dreset;
+    M.cfg.godunov = muscl ? MGPU_GODUNOV_PLM_MUSCL : MGPU_GODUNOV_PLM_SPLIT;
+    M.have_godunov = 1;
     changed();
     return 0;
   }
-  if (strcmp(key, "plm-muscl") == 0 || strcmp(key, "weno-split") == 0)
-    return luaL_error(L, "[Mara] integration scheme '%s' is not provided by the GPU module (only 'plm-split')",
-                      key);
+  if (strcmp(key, "weno-split") == 0)
+    return luaL_error(L, "[Mara] integration scheme '%s' is not provided by the GPU module "
+                         "(only 'plm-split' and 'plm-muscl')", key);
   return luaL_error(L, "[Mara] no such integration scheme '%s'", key);
 }
 
@@ -278,6 +288,7 @@ static int l_config_solver(lua_State *L)
   if (lua_isnumber(L, -1)) {
     M.cfg.theta = lua_tonumber(L, -1);
     if (!quiet) printf("[Mara] setting theta=%f\n", M.cfg.theta);
+    if (M.have_godunov && M.cfg.godunov == MGPU_GODUNOV_PLM_MUSCL) ctu_theta = M.cfg.theta;
   }
   lua_pop(L, 1);
 

@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import ctypes
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -31,6 +31,7 @@ RIEMANN = {"hll": 0, "hllc": 1, "hlld": 2}
 ADVANCE = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}
 IS_MODE = {"js96": 0, "b08": 1, "sz10": 2}
 PRECISION = {"fp64": 0, "fp32": 1}
+GODUNOV = {"plm-split": 0, "plm-muscl": 1}   # method of lines / CTU-Hancock
 PRIM_NAMES = ["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]   # Mara/rmhd.cpp:72-78
 
 
@@ -58,6 +59,7 @@ class Scheme:
     dreset: float = 1.0
     precision: str = "fp64"
     learned_c2p: bool = False
+    godunov: str = "plm-split"   # 'plm-muscl': CTU-Hancock with PLM slopes of limiter theta
 
     def to_config(self) -> _lib.MgpuConfig:
         lib = _lib.load()
@@ -76,6 +78,7 @@ class Scheme:
         c.dreset = self.dreset
         c.precision = PRECISION[self.precision]
         c.learned_c2p = int(self.learned_c2p)
+        c.godunov = GODUNOV[self.godunov]
         return c
 
 
@@ -202,7 +205,7 @@ class Solver:
         self._check(self.lib.mgpu_max_lorentz_factor(self.h, ctypes.byref(w)))
         return w.value
 
-    KERNEL_CLASSES = ["begin", "p2c", "c2p", "flux", "update"]
+    KERNEL_CLASSES = ["begin", "p2c", "c2p", "flux", "update", "predict"]
 
     def profile_enable(self, capacity: int = 4096):
         self._check(self.lib.mgpu_profile_enable(self.h, int(capacity)))
@@ -212,9 +215,10 @@ class Solver:
 
     def profile_read(self) -> dict:
         """Per kernel class: summed ms, launches and work units since the last read."""
-        ms = (ctypes.c_double * 5)()
-        ln = (ctypes.c_longlong * 5)()
-        un = (ctypes.c_longlong * 5)()
+        k = len(self.KERNEL_CLASSES)
+        ms = (ctypes.c_double * k)()
+        ln = (ctypes.c_longlong * k)()
+        un = (ctypes.c_longlong * k)()
         self._check(self.lib.mgpu_profile_read(self.h, ms, ln, un))
         return {k: {"ms": ms[i], "launches": ln[i], "units": un[i]}
                 for i, k in enumerate(self.KERNEL_CLASSES)}
@@ -287,6 +291,8 @@ class _Fluid:
 class MaraModule:
     """The ``Mara`` table of the reference (Mara/mara.cpp:137-268), GPU-backed."""
 
+    _ctu_theta = 2.0   # PlmCtuHancockOperator's plm_theta: process-wide, survives start()
+
     def __init__(self):
         self._reset()
         self.measure = _Measure(self)
@@ -352,10 +358,19 @@ class MaraModule:
         self._invalidate()
 
     def set_godunov(self, key: str):
+        """luaC_set_godunov (Mara/mara.cpp:960-984).  A new operator carries the constructor's
+        emergency-reset settings; 'plm-muscl' (CTU-Hancock) keeps its own limiter parameter,
+        a process-wide static changed only by config_solver{theta} while it is the current
+        operator (Mara/ctu-hancock.cpp:11, Mara/mara.cpp:1068-1074)."""
         self._need_start()
-        if key != "plm-split":
+        if key == "weno-split":
+            raise MaraError("[Mara] integration scheme 'weno-split' is not provided by the B200 module")
+        if key not in GODUNOV:
             raise MaraError(f"[Mara] no such integration scheme '{key}'")
+        d = Scheme()
+        self._scheme.ereset, self._scheme.preset, self._scheme.dreset = d.ereset, d.preset, d.dreset
         self._godunov = key
+        self._invalidate()
 
     def set_advance(self, key: str):
         self._need_start()
@@ -374,6 +389,8 @@ class MaraModule:
             s.extrap = tbl["extrap"]
         if "theta" in tbl:
             s.theta = float(tbl["theta"])
+            if self._godunov == "plm-muscl":
+                MaraModule._ctu_theta = s.theta
         if "IS" in tbl:
             if tbl["IS"] not in IS_MODE:
                 raise MaraError(f"no such IS: {tbl['IS']}")
@@ -412,7 +429,10 @@ class MaraModule:
             raise MaraError("[Mara] need a domain to run this, use set_domain")
         if self._s is None:
             x0, x1, N, Ng = self._domain
-            self._s = Solver(self._scheme, N, x0, x1, Ng)
+            scheme = replace(self._scheme, godunov=self._godunov or "plm-split")
+            if scheme.godunov == "plm-muscl":
+                scheme.theta = MaraModule._ctu_theta
+            self._s = Solver(scheme, N, x0, x1, Ng)
         return self._s
 
     # state -------------------------------------------------------------------------------

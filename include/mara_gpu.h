@@ -28,6 +28,8 @@ enum { MGPU_RECON_PCM = 0, MGPU_RECON_PLM = 1, MGPU_RECON_WENO5 = 2 };
 enum { MGPU_RIEMANN_HLL = 0, MGPU_RIEMANN_HLLC = 1, MGPU_RIEMANN_HLLD = 2 };
 enum { MGPU_IS_JS96 = 0, MGPU_IS_B08 = 1, MGPU_IS_SZ10 = 2 };
 enum { MGPU_PREC_FP64 = 0, MGPU_PREC_FP32 = 1 };
+enum { MGPU_GODUNOV_PLM_SPLIT = 0, MGPU_GODUNOV_PLM_MUSCL = 1 };
+#define MGPU_KERNEL_CLASSES 6
 
 /* Solver selection: the union of Mara.set_fluid/set_eos/set_godunov/set_riemann/set_advance
  * and the keys of Mara.config_solver (Mara/mara.cpp:813-1167). */
@@ -48,6 +50,12 @@ typedef struct {
                           MGPU_PREC_FP32: FP32 bulk, FP64 c2p polish / magnetic field / dt */
   int    learned_c2p;  /* 1: first c2p attempt starts from the network set by
                           mgpu_set_c2p_network (Newton polish, reference ladder as fallback) */
+  int    godunov;      /* set_godunov: MGPU_GODUNOV_PLM_SPLIT 'plm-split' (method of lines,
+                          reconstruction `recon`, MethodOfLinesSplit, Mara/plm-split.cpp) or
+                          MGPU_GODUNOV_PLM_MUSCL 'plm-muscl' (CTU-Hancock with PLM slopes of
+                          limiter `theta`, PlmCtuHancockOperator, Mara/ctu-hancock.cpp:53-494;
+                          single domains only: not with external guards, ensembles or
+                          mgpu_advance_noalloc) */
 } mgpu_config;
 
 typedef struct {
@@ -118,10 +126,12 @@ int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax);
 int mgpu_measure_divB_state(mgpu_solver *h, double *mean, double *max);
 
 /* Kernel timing (no counterpart in the reference): while enabled, every kernel launch of an
- * advance is bracketed by CUDA events on the handle's stream.  Classes: 0 begin/commit,
- * 1 P->U, 2 c2p, 3 flux sweep, 4 CT+divergence+RK update.  mgpu_profile_read synchronizes
- * and returns per class the summed milliseconds, the number of launches and the work units
- * (faces for the flux class, interior zones otherwise); it then starts a new window. */
+ * advance is bracketed by CUDA events on the handle's stream.  Classes (MGPU_KERNEL_CLASSES):
+ * 0 begin/commit, 1 P->U, 2 c2p, 3 flux sweep, 4 CT+divergence+RK update, 5 CTU-Hancock
+ * predictor (half-step states and their c2p).  mgpu_profile_read synchronizes and returns per
+ * class, in arrays of MGPU_KERNEL_CLASSES entries, the summed milliseconds, the number of
+ * launches and the work units (faces for the flux class, zones otherwise); it then starts a
+ * new window. */
 int mgpu_profile_enable(mgpu_solver *h, int capacity);
 int mgpu_profile_disable(mgpu_solver *h);
 int mgpu_profile_read(mgpu_solver *h, double *ms, long long *launches, long long *units);

@@ -57,7 +57,17 @@ STEP_CASES = {
                                 advance="single"), lambda: _line((24,), seed=20), 6, 0.3),
     "ctu_fail_8": (dict(n=(8, 7, 6), godunov="plm-muscl", riemann="hllc", advance="rk2"),
                    lambda: ics.turbulence_box((8, 7, 6), seed=1, vrms=0.4), 6, 0.4),
+    # a zone with p < 0 under config_solver{ereset}: the stage c2p resets it and the operator
+    # runs on P->U of the repaired primitives
+    "ctu_ereset_8": (dict(n=(8, 8, 8), godunov="plm-muscl", ereset=True, preset=0.5, dreset=2.0),
+                     lambda: _bad_zone((8, 8, 8), seed=3), 3, 0.3),
 }
+
+
+def _bad_zone(n, seed):
+    P = ics.turbulence_box(n, seed=seed)
+    P[5, 5, 5, 1] = -1.0
+    return P
 
 
 def _line(n, seed):

@@ -26,10 +26,13 @@ DT_TOL = 1e-12          # relative, dt and MaxLambda
 # 1.7e-7 (PLM+HLLC) and 5.5e-8 (WENO5+HLLD) there.  CUDA's transcendentals differ from
 # glibc's by such ulps, so the bound for those fixtures is set from the measured
 # sensitivity (x6) instead of 1e-10.
-CASE_TOL = {"kh2d_plm_hllc_rk3": 1e-6, "kh2d_weno5_hlld_rk2": 1e-6}
+CASE_TOL = {"kh2d_plm_hllc_rk3": 1e-6, "kh2d_weno5_hlld_rk2": 1e-6, "ctu_kh2d_hllc_rk3": 3e-6}
 
 STEP_CASES = ["plm_hlld_rk2_8", "weno5_hlld_rk3_8", "plm_hllc_rk3_odd", "pcm_hll_rk4_6",
-              "kh2d_plm_hllc_rk3", "kh2d_weno5_hlld_rk2", "hllc_fail_12"]
+              "kh2d_plm_hllc_rk3", "kh2d_weno5_hlld_rk2", "hllc_fail_12",
+              # CTU-Hancock (set_godunov('plm-muscl'))
+              "ctu_plm_hlld_single_8", "ctu_hll_rk2_odd", "ctu_kh2d_hllc_rk3", "ctu_1d_hlld_single",
+              "ctu_fail_8", "ctu_ereset_8"]
 
 
 def rel_linf(a, b):

@@ -15,7 +15,7 @@ STEP_CASES = ["plm_hlld_rk2_8", "weno5_hlld_rk3_8", "plm_hllc_rk3_odd", "pcm_hll
               "kh2d_plm_hllc_rk3", "kh2d_weno5_hlld_rk2", "hllc_fail_12",
               # CTU-Hancock (plm-muscl)
               "ctu_plm_hlld_single_8", "ctu_hll_rk2_odd", "ctu_kh2d_hllc_rk3", "ctu_1d_hlld_single",
-              "ctu_fail_8"]
+              "ctu_fail_8", "ctu_ereset_8"]
 
 
 @pytest.mark.parametrize("case", STEP_CASES)

@@ -213,183 +213,6 @@ struct TcNet {
   }
 };
 
-// Two tiles in flight per CTA: while the tensor cores run one tile's layer, the threads run
-// the other tile's epilogue.  Each tile has its own operand buffer, TMEM columns (64 each)
-// and mbarrier; every thread owns row r of both tiles.
-constexpr int SMEM2_BYTES = 1024 + IMAGE_SLOT + 2 * A_BYTES + 64;
-constexpr int TMEM2_COLS = 128;
-
-struct TcNet2 {
-  unsigned char *img;
-  unsigned char *A[2];
-  uint32_t mbar[2];
-  uint32_t tmem[2];
-  uint32_t phase[2];
-  int pending[2];          // a commit of tile t not yet waited for successfully
-  uint32_t pend_parity[2]; // ... and the parity that completes it
-  int ok;
-
-  // smem writes of the operands visible to the tensor cores; TMEM reads ordered before
-  __device__ __forceinline__ void sync_for_issue() const
-  {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  }
-
-  // one elected thread issues D_t = A_t * W^T (K in steps of 16) and commits to mbar[t];
-  // every thread records the pending commit
-  __device__ __forceinline__ void issue(int t, uint32_t w_addr, int K, int N)
-  {
-    pending[t] = 1;
-    pend_parity[t] = phase[t];
-    if (threadIdx.x == 0) {
-      const uint32_t a_addr = smem_u32(A[t]);
-      const uint32_t id = idesc_bf16(N);
-      for (int s = 0; s < K / 16; ++s)
-        mma_bf16(tmem[t], sdesc(a_addr + 256 * s, 128, K * 16), sdesc(w_addr + 256 * s, 128, K * 16), id, s > 0);
-      mma_commit(mbar[t]);
-    }
-  }
-
-  // all threads wait for tile t's MMAs (bounded); false once any wait timed out
-  __device__ __forceinline__ bool wait(int t)
-  {
-    const bool done = mbar_wait(mbar[t], phase[t]);
-    phase[t] ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool all = __syncthreads_and(done) != 0;
-    if (all) pending[t] = 0;
-    else ok = 0;
-    return all;
-  }
-
-  __device__ __forceinline__ void epilogue(int t, const float *bias)
-  {
-    const int r = threadIdx.x, warp = r >> 5;
-    const uint32_t row = tmem[t] + ((uint32_t) (warp * 32) << 16);
-#pragma unroll 1
-    for (int c0 = 0; c0 < 64; c0 += 16) {
-      float v[16];
-      tmem_ld16(row + (uint32_t) c0, v);
-      uint32_t h[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-        h[i] = tanh_bf16x2(pack_bf16x2(v[2 * i] + bias[c0 + 2 * i], v[2 * i + 1] + bias[c0 + 2 * i + 1]));
-      *reinterpret_cast<uint4 *>(A[t] + canon_offset(r, c0, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4 *>(A[t] + canon_offset(r, c0 + 8, 64)) = make_uint4(h[4], h[5], h[6], h[7]);
-    }
-  }
-
-  __device__ __forceinline__ void input(int t, const float *xn)
-  {
-    float v[8] = {xn[0], xn[1], xn[2], xn[3], xn[4], 0.f, 0.f, 0.f};
-    const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    store_chunk(A[t], threadIdx.x, 0, 16, v);
-    store_chunk(A[t], threadIdx.x, 1, 16, z);
-  }
-
-  __device__ __forceinline__ void output(int t, float *y) const
-  {
-    const float *f = reinterpret_cast<const float *>(img + F_OFF);
-    float v[16];
-    tmem_ld16(tmem[t] + ((uint32_t) ((threadIdx.x >> 5) * 32) << 16), v);
-    y[0] = (v[0] + f[F_B4 + 0]) * f[F_YS + 0] + f[F_YM + 0];
-    y[1] = (v[1] + f[F_B4 + 1]) * f[F_YS + 1] + f[F_YM + 1];
-  }
-
-  // Both tiles' forward passes, interleaved layer by layer.  False if the CTA has stopped
-  // using the tensor cores (then y is not written).
-  __device__ __forceinline__ bool forward2(const float *xa, const float *xb, float *ya, float *yb)
-  {
-    if (!ok) return false;
-    const float *f = reinterpret_cast<const float *>(img + F_OFF);
-    const uint32_t w = smem_u32(img);
-    const uint32_t wl[4] = {w + W1_OFF, w + W2_OFF, w + W3_OFF, w + W4_OFF};
-    const int Kl[4] = {16, 64, 64, 64}, Nl[4] = {64, 64, 64, 16};
-    const float *bl[3] = {f + F_B1, f + F_B2, f + F_B3};
-    input(0, xa);
-    input(1, xb);
-    sync_for_issue();
-    issue(0, wl[0], Kl[0], Nl[0]);
-    issue(1, wl[0], Kl[0], Nl[0]);
-#pragma unroll 1
-    for (int l = 0; l < 3; ++l) {
-      for (int t = 0; t < 2; ++t) {
-        if (!wait(t)) return false;
-        epilogue(t, bl[l]);
-        sync_for_issue();
-        issue(t, wl[l + 1], Kl[l + 1], Nl[l + 1]);
-      }
-    }
-    if (!wait(0)) return false;
-    output(0, ya);
-    if (!wait(1)) return false;
-    output(1, yb);
-    // every thread's TMEM reads complete before the next pair's first MMAs overwrite them
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    return true;
-  }
-
-  __device__ __forceinline__ void normalise(const float *x, float *xn) const
-  {
-    const float *f = reinterpret_cast<const float *>(img + F_OFF);
-#pragma unroll
-    for (int i = 0; i < 5; ++i) xn[i] = (x[i] - f[F_XM + i]) / f[F_XS + i];
-  }
-};
-
-__device__ __forceinline__ TcNet2 tc_setup2(unsigned char *smem, const unsigned char *image)
-{
-  TcNet2 n;
-  unsigned char *base = (unsigned char *) (((uintptr_t) smem + 1023) & ~(uintptr_t) 1023);
-  n.img = base;
-  n.A[0] = base + IMAGE_SLOT;
-  n.A[1] = n.A[0] + A_BYTES;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(n.A[1] + A_BYTES);
-  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
-  for (int i = threadIdx.x; i < IMAGE_BYTES / 16; i += blockDim.x)
-    reinterpret_cast<uint4 *>(n.img)[i] = reinterpret_cast<const uint4 *>(image)[i];
-  n.mbar[0] = smem_u32(bar);
-  n.mbar[1] = smem_u32(bar + 1);
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(n.mbar[0]) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(n.mbar[1]) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (threadIdx.x < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-                 "r"(TMEM2_COLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  n.tmem[0] = *slot;
-  n.tmem[1] = *slot + 64;   // columns 64..127
-  n.phase[0] = n.phase[1] = 0;
-  n.pending[0] = n.pending[1] = 0;
-  n.pend_parity[0] = n.pend_parity[1] = 0;
-  n.ok = 1;
-  return n;
-}
-
-// Release TMEM; after a timed-out wait, first wait once more (bounded) for every commit still
-// pending, so no MMA writes TMEM after the dealloc.
-__device__ __forceinline__ void tc_teardown2(TcNet2 &n)
-{
-  for (int t = 0; t < 2; ++t)
-    if (n.pending[t]) mbar_wait(n.mbar[t], n.pend_parity[t]);
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(n.tmem[0]), "r"(TMEM2_COLS) : "memory");
-}
-
 // Set-up: copy the network image to shared memory, allocate TMEM, initialise the mbarrier.
 // `smem` is the CTA's dynamic shared memory (SMEM_BYTES).
 __device__ __forceinline__ TcNet tc_setup(unsigned char *smem, const unsigned char *image)

@@ -12,14 +12,6 @@
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
 #endif
-// Two 128-zone tiles in flight per CTA of the tensor-core c2p (1), or one (0); the paired
-// kernel's 55 KB of shared memory allows 3 CTAs per SM.
-#ifndef MGPU_TC_PAIRS
-#define MGPU_TC_PAIRS 1
-#endif
-#ifndef MGPU_TC2_CTAS_PER_SM
-#define MGPU_TC2_CTAS_PER_SM 3
-#endif
 
 namespace mgpu {
 
@@ -89,19 +81,7 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
     const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
-    if (tc_c2p && MGPU_TC_PAIRS) {
-      static bool smem_set = false;   // 55 KB of dynamic shared memory needs the opt-in
-      if (!smem_set) {
-        const cudaError_t e = cudaFuncSetAttribute(k_cons_to_prim_tc2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   tc::SMEM2_BYTES);
-        if (e != cudaSuccess) return e;
-        smem_set = true;
-      }
-      const long long npairs = (g.ninterior + 255) / 256;
-      const long long pmax = 148ll * MGPU_TC2_CTAS_PER_SM;
-      k_cons_to_prim_tc2<T><<<(unsigned) (npairs < pmax ? npairs : pmax), 128, tc::SMEM2_BYTES, st>>>(
-          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
-    } else if (tc_c2p)
+    if (tc_c2p)
       k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
                                                                 final, A.ereset, A.preset, A.dreset);
     else if (simt_net)

@@ -15,9 +15,6 @@ namespace mgpu {
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
 #endif
-#ifndef MGPU_TC2_CTAS_PER_SM
-#define MGPU_TC2_CTAS_PER_SM 3
-#endif
 
 template <class T>
 __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
@@ -66,77 +63,6 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
   }
   if (!net.ok && threadIdx.x == 0) atomicExch(&ctl->tc_fault, 1);
   tc::tc_teardown(net);
-}
-
-// The same with two tiles in flight per CTA (TcNet2): tile pair p covers zones
-// [256 p, 256 p + 256); thread r owns row r of both tiles.  The network runs for both tiles
-// interleaved, then each thread polishes and scatters its two zones.
-template <class T>
-__device__ __forceinline__ void tc2_features(const Grid &g, StateCPtr<T> U, const T *PA, int zero_guess,
-                                             const tc::TcNet2 &net, long long t, float *xn, bool &good)
-{
-  xn[0] = xn[1] = xn[2] = xn[3] = xn[4] = 0.f;
-  good = false;
-  if (t >= g.ninterior) return;
-  int i, j, k;
-  interior_coords(g, t, i, j, k);
-  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-  double u[8];
-  load_state(g, U, z, u);
-  if (check_cons(u) != C2P_SUCCESS) return;
-  const double S2 = u[Sx] * u[Sx] + u[Sy] * u[Sy] + u[Sz] * u[Sz];
-  const double B2 = u[Bx] * u[Bx] + u[By] * u[By] + u[Bz] * u[Bz];
-  const double BS = u[Bx] * u[Sx] + u[By] * u[Sy] + u[Bz] * u[Sz];
-  float x[5];
-  c2p_features(u[ddd], u[tau], S2, B2, BS * BS, x);
-  net.normalise(x, xn);
-  good = isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]) && isfinite(xn[3]) && isfinite(xn[4]);
-  if (!good) xn[0] = xn[1] = xn[2] = xn[3] = xn[4] = 0.f;
-}
-
-template <class T>
-__device__ __forceinline__ void tc2_polish(const Grid &g, StateCPtr<T> U, T *PA, StatePtr<T> Pn, const PhysParams &pp,
-                                           Ctl *ctl, int stage, int zero_guess, int final, int ereset, double preset,
-                                           double dreset, long long t, bool have, bool good, const float *y)
-{
-  if (t >= g.ninterior) return;
-  int i, j, k;
-  interior_coords(g, t, i, j, k);
-  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-  double u[8], p[8];
-  load_state(g, U, z, u);
-#pragma unroll
-  for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
-  double Zg = 0.0, Wg = 0.0;
-  const bool use = have && good && c2p_guess_from_output(u[ddd], y, Zg, Wg);
-  C2PTally tally;
-  const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
-  c2p_finish<T>(g, PA, Pn, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err, tally);
-}
-
-template <class T>
-__global__ void __launch_bounds__(128, MGPU_TC2_CTAS_PER_SM) k_cons_to_prim_tc2(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
-                                                          StatePtr<T> Pn1, PhysParams pp, Ctl *ctl, int stage,
-                                                          int zero_guess, int final, int ereset, double preset,
-                                                          double dreset)
-{
-  if (stage_failed(ctl, stage)) return;
-  extern __shared__ unsigned char tc_smem[];
-  tc::TcNet2 net = tc::tc_setup2(tc_smem, (const unsigned char *) pp.mlp_tc);
-  const StatePtr<T> Pn = ctl->cur ? Pn0 : Pn1;
-  const long long npairs = (g.ninterior + 255) / 256;
-  for (long long pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
-    const long long ta = pair * 256 + threadIdx.x, tb = ta + 128;
-    float xa[5], xb[5], ya[2] = {0.f, 0.f}, yb[2] = {0.f, 0.f};
-    bool ga, gb;
-    tc2_features<T>(g, U, PA, zero_guess, net, ta, xa, ga);
-    tc2_features<T>(g, U, PA, zero_guess, net, tb, xb, gb);
-    const bool have = net.forward2(xa, xb, ya, yb);
-    tc2_polish<T>(g, U, PA, Pn, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, ta, have, ga, ya);
-    tc2_polish<T>(g, U, PA, Pn, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, tb, have, gb, yb);
-  }
-  if (!net.ok && threadIdx.x == 0) atomicExch(&ctl->tc_fault, 1);
-  tc::tc_teardown2(net);
 }
 
 }  // namespace mgpu

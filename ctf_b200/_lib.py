@@ -23,7 +23,8 @@ class MgpuConfig(ctypes.Structure):
                 ("theta", ctypes.c_double), ("is_mode", ctypes.c_int), ("sz10A", ctypes.c_double),
                 ("riemann", ctypes.c_int), ("rk", ctypes.c_int), ("pfloor", ctypes.c_double),
                 ("ereset", ctypes.c_int), ("preset", ctypes.c_double), ("dreset", ctypes.c_double),
-                ("precision", ctypes.c_int), ("learned_c2p", ctypes.c_int), ("godunov", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("learned_c2p", ctypes.c_int), ("godunov", ctypes.c_int),
+                ("layout", ctypes.c_int)]
 
 
 class MgpuStats(ctypes.Structure):
@@ -64,6 +65,8 @@ SIGNATURES = {
     "mgpu_download_prim": (ctypes.c_int, [_vp, _dp]),
     "mgpu_upload_prim_device": (ctypes.c_int, [_vp, _vp]),
     "mgpu_download_prim_device": (ctypes.c_int, [_vp, _vp]),
+    "mgpu_upload_prim_range": (ctypes.c_int, [_vp, _dp, ctypes.c_longlong, ctypes.c_longlong]),
+    "mgpu_download_prim_range": (ctypes.c_int, [_vp, _dp, ctypes.c_longlong, ctypes.c_longlong]),
     "mgpu_advance": (ctypes.c_int, [_vp, ctypes.c_double, _ip]),
     "mgpu_advance_host": (ctypes.c_int, [_vp, _dp, ctypes.c_double, _dp, _ip]),
     "mgpu_advance_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,

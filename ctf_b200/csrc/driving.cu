@@ -25,6 +25,8 @@
 #include <vector>
 
 #include "solver.h"
+#include "c2p_mlp.cuh"
+#include "rmhd_physics.cuh"
 
 using namespace mgpu;
 
@@ -121,7 +123,8 @@ struct MgpuDriving {
   double P0 = 0, zeta = 0;
   std::vector<std::complex<double>> K[3], F[3];
   std::vector<OuProcess> proc;
-  double *dev_F = nullptr;          // sampled field, 3 x nz doubles (device)
+  void *dev_F = nullptr;            // sampled field, 3 x nz doubles (floats in the lean layout)
+  int f32 = 0;                      // dev_F holds floats
   double2 *dev_modes = nullptr;     // F_m per component, 3 x numk (device)
   double2 *dev_phase = nullptr;     // per-axis phases e^{i 2 pi a x_i}: 3 x (2k1+1) x G_max
   int gmax = 0;
@@ -248,8 +251,9 @@ int fail(mgpu_solver *h, int code, const char *msg)
 
 // F(x) at every guarded zone (DrivingProcedure::ResampleField, Mara/driving.cpp:44-84):
 // zone coordinates x_at(i) = x0 + dx (i - Ng + 1/2), guards included.
+template <class FT>
 __global__ void k_drive_sample(Grid g, int nd, int k1, const double2 *modes, const double2 *phase, int gmax,
-                               double *F)
+                               FT *F)
 {
   const int r = 2 * k1 + 1;
   const int numk = nd == 3 ? r * r * r : r * r;
@@ -282,13 +286,36 @@ __global__ void k_drive_sample(Grid g, int nd, int k1, const double2 *modes, con
         }
       }
     }
-    for (int q = 0; q < 3; ++q) F[q * g.nz + z] = acc[q];
+    for (int q = 0; q < 3; ++q) F[q * g.nz + z] = FT(acc[q]);
   }
 }
 
-// The 4-velocity kick of Drive_rmhd on the committed state, every guarded zone, only if the
-// advance committed.  In 2D the reference kicks vx, vy and carries vz as given (its
-// 4-velocity array holds the 3-velocity vz there).
+// The 4-velocity kick of Drive_rmhd on one zone's primitives p (rho, vx, vy, vz updated).
+// In 2D the reference kicks vx, vy and carries vz as given (its 4-velocity array holds the
+// 3-velocity vz there).
+template <class FT>
+__device__ __forceinline__ void drive_kick_zone(const Grid &g, int nd, const FT *F, long long z, double dt, double *p)
+{
+  double uf[4] = {0.0, p[vx], p[vy], p[vz]};
+  const double v2 = uf[1] * uf[1] + uf[2] * uf[2] + uf[3] * uf[3];
+  const double W0 = 1.0 / sqrt(1.0 - v2);
+  uf[1] *= W0;
+  uf[1] += double(F[0 * g.nz + z]) * (dt / W0);
+  uf[2] *= W0;
+  uf[2] += double(F[1 * g.nz + z]) * (dt / W0);
+  if (nd == 3) {
+    uf[3] *= W0;
+    uf[3] += double(F[2 * g.nz + z]) * (dt / W0);
+  }
+  const double u2 = uf[1] * uf[1] + uf[2] * uf[2] + uf[3] * uf[3];
+  const double W1 = sqrt(1.0 + u2);
+  p[vx] = uf[1] / W1;
+  p[vy] = uf[2] / W1;
+  p[vz] = uf[3] / W1;
+  p[rho] = p[rho] * (W0 / W1);
+}
+
+// The kick on the committed state, every guarded zone, only if the advance committed.
 template <class T>
 __global__ void k_drive_kick(Grid g, int nd, const double *F, T *bulk0, T *bulk1, const Ctl *ctl)
 {
@@ -297,27 +324,49 @@ __global__ void k_drive_kick(Grid g, int nd, const double *F, T *bulk0, T *bulk1
   const double dt = ctl->dt;
   for (long long z = (long long) blockIdx.x * blockDim.x + threadIdx.x; z < g.nz;
        z += (long long) gridDim.x * blockDim.x) {
-    double uf[4] = {0.0, double(P[vx * g.cs + z]), double(P[vy * g.cs + z]), double(P[vz * g.cs + z])};
-    const double v2 = uf[1] * uf[1] + uf[2] * uf[2] + uf[3] * uf[3];
-    const double W0 = 1.0 / sqrt(1.0 - v2);
-    uf[1] *= W0;
-    uf[1] += F[0 * g.nz + z] * (dt / W0);
-    uf[2] *= W0;
-    uf[2] += F[1 * g.nz + z] * (dt / W0);
-    if (nd == 3) {
-      uf[3] *= W0;
-      uf[3] += F[2 * g.nz + z] * (dt / W0);
-    }
-    const double u2 = uf[1] * uf[1] + uf[2] * uf[2] + uf[3] * uf[3];
-    const double W1 = sqrt(1.0 + u2);
-    P[vx * g.cs + z] = T(uf[1] / W1);
-    P[vy * g.cs + z] = T(uf[2] / W1);
-    P[vz * g.cs + z] = T(uf[3] / W1);
-    P[rho * g.cs + z] = T(double(P[rho * g.cs + z]) * (W0 / W1));
+    double p[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) p[q] = double(P[q * g.cs + z]);
+    drive_kick_zone<double>(g, nd, F, z, dt, p);
+    P[vx * g.cs + z] = T(p[vx]);
+    P[vy * g.cs + z] = T(p[vy]);
+    P[vz * g.cs + z] = T(p[vz]);
+    P[rho * g.cs + z] = T(p[rho]);
+  }
+}
+
+// The kick in the lean layout: the committed primitives are PA, every guarded zone; the
+// committed conserved state U[cur] is rebuilt from the kicked primitives at interior zones
+// (the next advance starts from it).
+template <class T, class FT>
+__global__ void k_drive_kick_lean(Grid g, int nd, const FT *F, T *PA, StatePtr<T> UA, StatePtr<T> UB, double gamma,
+                                  const Ctl *ctl)
+{
+  if (!ctl->committed) return;
+  const StatePtr<T> U = ctl->cur ? UB : UA;
+  const double dt = ctl->dt;
+  for (long long z = (long long) blockIdx.x * blockDim.x + threadIdx.x; z < g.nz;
+       z += (long long) gridDim.x * blockDim.x) {
+    double p[8], u[8];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) p[q] = double(PA[q * g.cs + z]);
+    drive_kick_zone<FT>(g, nd, F, z, dt, p);
+    PA[vx * g.cs + z] = T(p[vx]);
+    PA[vy * g.cs + z] = T(p[vy]);
+    PA[vz * g.cs + z] = T(p[vz]);
+    PA[rho * g.cs + z] = T(p[rho]);
+    const int i = (int) (z / g.s[0]), j = (int) ((z / g.s[1]) % g.G[1]), k = (int) (z % g.G[2]);
+    if (i < g.ng || i >= g.ng + g.n[0] || j < g.ng || j >= g.ng + g.n[1] || k < g.ng || k >= g.ng + g.n[2]) continue;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) p[5 + q] = U.B[q * g.cs + z];
+    prim_to_cons(gamma, p, u);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) U.bulk[q * g.cs + z] = T(u[q]);
   }
 }
 
 bool fp32(const mgpu_solver *h) { return h->cfg.precision == MGPU_PREC_FP32; }
+bool lean(const mgpu_solver *h) { return h->cfg.layout == MGPU_LAYOUT_LEAN; }
 
 int resample(mgpu_solver *h)
 {
@@ -343,7 +392,12 @@ int resample(mgpu_solver *h)
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(D.dev_modes, modes.data(), modes.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) {
-    k_drive_sample<<<148 * 8, 256, 0, h->stream>>>(g, D.nd, D.k1, D.dev_modes, D.dev_phase, D.gmax, D.dev_F);
+    if (D.f32)
+      k_drive_sample<float><<<148 * 8, 256, 0, h->stream>>>(g, D.nd, D.k1, D.dev_modes, D.dev_phase, D.gmax,
+                                                            (float *) D.dev_F);
+    else
+      k_drive_sample<double><<<148 * 8, 256, 0, h->stream>>>(g, D.nd, D.k1, D.dev_modes, D.dev_phase, D.gmax,
+                                                             (double *) D.dev_F);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);   // host vectors die here
@@ -360,11 +414,24 @@ cudaError_t mgpu_driving_enqueue(mgpu_solver *h)
 {
   if (!h->driving) return cudaSuccess;
   const Grid &g = h->g;
+  const MgpuDriving &D = *h->driving;
+  const AdvanceBuffers &b = h->b;
+  if (lean(h)) {
+    if (fp32(h))
+      k_drive_kick_lean<float, float><<<148 * 8, 256, 0, h->stream>>>(
+          g, D.nd, (const float *) D.dev_F, (float *) b.PA, StatePtr<float>{(float *) b.U0_bulk, b.U0_B},
+          StatePtr<float>{(float *) b.U1_bulk, b.U1_B}, h->cfg.gamma, h->ctl);
+    else
+      k_drive_kick_lean<double, float><<<148 * 8, 256, 0, h->stream>>>(
+          g, D.nd, (const float *) D.dev_F, (double *) b.PA, StatePtr<double>{(double *) b.U0_bulk, b.U0_B},
+          StatePtr<double>{(double *) b.U1_bulk, b.U1_B}, h->cfg.gamma, h->ctl);
+    return cudaGetLastError();
+  }
   if (fp32(h))
-    k_drive_kick<float><<<148 * 8, 256, 0, h->stream>>>(g, h->driving->nd, h->driving->dev_F,
+    k_drive_kick<float><<<148 * 8, 256, 0, h->stream>>>(g, h->driving->nd, (const double *) h->driving->dev_F,
                                                         (float *) h->b.Pc_bulk[0], (float *) h->b.Pc_bulk[1], h->ctl);
   else
-    k_drive_kick<double><<<148 * 8, 256, 0, h->stream>>>(g, h->driving->nd, h->driving->dev_F,
+    k_drive_kick<double><<<148 * 8, 256, 0, h->stream>>>(g, h->driving->nd, (const double *) h->driving->dev_F,
                                                          (double *) h->b.Pc_bulk[0], (double *) h->b.Pc_bulk[1], h->ctl);
   return cudaGetLastError();
 }
@@ -421,7 +488,8 @@ int mgpu_set_driving(mgpu_solver *h, const void *field, long long bytes)
   }
   const Grid &g = h->g;
   D->gmax = g.G[0] > g.G[1] ? (g.G[0] > g.G[2] ? g.G[0] : g.G[2]) : (g.G[1] > g.G[2] ? g.G[1] : g.G[2]);
-  cudaError_t e = cudaMalloc((void **) &D->dev_F, sizeof(double) * 3 * (size_t) g.nz);
+  D->f32 = lean(h);   // the lean layout's boxes keep the sampled field in FP32 (12 B per zone)
+  cudaError_t e = cudaMalloc(&D->dev_F, (D->f32 ? sizeof(float) : sizeof(double)) * 3 * (size_t) g.nz);
   if (e == cudaSuccess) e = cudaMalloc((void **) &D->dev_modes, sizeof(double2) * 3 * (size_t) D->numk);
   if (e == cudaSuccess) e = cudaMalloc((void **) &D->dev_phase, sizeof(double2) * 3 * (size_t) D->rank() * D->gmax);
   if (e != cudaSuccess) {
@@ -473,16 +541,27 @@ int mgpu_driving_power(mgpu_solver *h, double *power)
   *power = 0.0;
   if (!h->driving) return MGPU_OK;
   const long long nz = h->g.nz;
-  std::vector<double> F((size_t) 3 * nz);
+  const MgpuDriving &D = *h->driving;
+  const size_t esz = D.f32 ? sizeof(float) : sizeof(double);
+  const long long chunk = 1ll << 22;   // zones per host copy
+  std::vector<unsigned char> buf((size_t) 3 * chunk * esz);
+  auto at = [&](int q, long long z) {
+    return D.f32 ? (double) ((const float *) buf.data())[q * chunk + z] : ((const double *) buf.data())[q * chunk + z];
+  };
   cudaError_t e = cudaStreamSynchronize(h->stream);
-  if (e == cudaSuccess) e = cudaMemcpy(F.data(), h->driving->dev_F, F.size() * sizeof(double), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, cudaGetErrorString(e));
   double s = 0.0;
-  for (long long z = 0; z < nz; ++z) {
-    double v = F[z] * F[z] + F[nz + z] * F[nz + z];
-    if (h->driving->nd == 3) v += F[2 * nz + z] * F[2 * nz + z];
-    s += v;
+  for (long long z0 = 0; z0 < nz && e == cudaSuccess; z0 += chunk) {
+    const long long cnt = nz - z0 < chunk ? nz - z0 : chunk;
+    for (int q = 0; q < D.nd && e == cudaSuccess; ++q)
+      e = cudaMemcpy(buf.data() + (size_t) q * chunk * esz, (const unsigned char *) D.dev_F + ((size_t) q * nz + z0) * esz,
+                     (size_t) cnt * esz, cudaMemcpyDeviceToHost);
+    for (long long z = 0; z < cnt && e == cudaSuccess; ++z) {
+      double v = at(0, z) * at(0, z) + at(1, z) * at(1, z);
+      if (D.nd == 3) v += at(2, z) * at(2, z);
+      s += v;
+    }
   }
+  if (e != cudaSuccess) return fail(h, MGPU_ERR_CUDA, cudaGetErrorString(e));
   *power = s / (double) nz;
   return MGPU_OK;
 }

@@ -382,6 +382,8 @@ int mgpu_ensemble_create(const mgpu_config *cfg, int nd, int nboxes, const int *
       (cfg->precision != MGPU_PREC_FP64 && cfg->precision != MGPU_PREC_FP32))
     return reject("bad configuration", MGPU_ERR_ARG);
   if (cfg->learned_c2p) return reject("the learned c2p guess is not offered for ensembles", MGPU_ERR_UNSUPPORTED);
+  if (cfg->layout != MGPU_LAYOUT_STANDARD)
+    return reject("ensembles use the standard layout", MGPU_ERR_UNSUPPORTED);
   if (cfg->godunov != MGPU_GODUNOV_PLM_SPLIT)
     return reject("ensembles use the method-of-lines operator (plm-split)", MGPU_ERR_UNSUPPORTED);
   if (nd < 1 || nd > 3) return reject("boxes must have 1, 2 or 3 dimensions", MGPU_ERR_ARG);

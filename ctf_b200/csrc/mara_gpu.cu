@@ -41,6 +41,7 @@ int cuda_fail(mgpu_solver *h, cudaError_t e, const char *where)
   } while (0)
 
 bool fp32(const mgpu_solver *h) { return h->cfg.precision == MGPU_PREC_FP32; }
+bool lean(const mgpu_solver *h) { return h->cfg.layout == MGPU_LAYOUT_LEAN; }
 
 PhysParams phys(const mgpu_solver *h)
 {
@@ -86,6 +87,8 @@ TransferArgs transfer_args(mgpu_solver *h)
   t.ctl = h->ctl;
   t.stream = h->stream;
   t.cur = 0;
+  t.lean = lean(h);
+  t.gamma = h->cfg.gamma;
   return t;
 }
 
@@ -219,6 +222,7 @@ int mgpu_default_config(mgpu_config *c)
   c->precision = MGPU_PREC_FP64;
   c->learned_c2p = 0;
   c->godunov = MGPU_GODUNOV_PLM_SPLIT;
+  c->layout = MGPU_LAYOUT_STANDARD;
   return MGPU_OK;
 }
 
@@ -234,6 +238,9 @@ static int check_config(mgpu_solver *h, const mgpu_config *c)
     return fail(h, MGPU_ERR_ARG, "no such precision");
   if (c->godunov != MGPU_GODUNOV_PLM_SPLIT && c->godunov != MGPU_GODUNOV_PLM_MUSCL)
     return fail(h, MGPU_ERR_ARG, "no such integration scheme");
+  if (c->layout != MGPU_LAYOUT_STANDARD && c->layout != MGPU_LAYOUT_LEAN) return fail(h, MGPU_ERR_ARG, "no such layout");
+  if (c->layout == MGPU_LAYOUT_LEAN && (c->godunov != MGPU_GODUNOV_PLM_SPLIT || c->rk > 3))
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs 'plm-split' with single, rk2 or rk3");
   return MGPU_OK;
 }
 
@@ -312,6 +319,7 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
   if (ng < 3) return fail(h, MGPU_ERR_ARG, "the step's stencils need Ng >= 3");
   for (int d = 0; d < nd; ++d)
     if (N[d] < ng) return fail(h, MGPU_ERR_ARG, "periodic guard fill needs N >= Ng on every axis");
+  if (lean(h) && nd != 3) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout is for 3D boxes");
   CK(cudaStreamSynchronize(h->stream));
   free_buffers(h);
   mgpu_driving_free(h);
@@ -356,16 +364,18 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
     return e;
   };
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = state(&h->b.Pc_bulk[i], &h->b.Pc_B[i]);
+  // lean layout: PA, the two conserved registers and the six transverse face fields only
+  for (int i = 0; i < 2 && e == cudaSuccess && !lean(h); ++i) e = state(&h->b.Pc_bulk[i], &h->b.Pc_B[i]);
   if (e == cudaSuccess) e = state(&h->b.U0_bulk, &h->b.U0_B);
   if (e == cudaSuccess) e = state(&h->b.U1_bulk, &h->b.U1_B);
   if (h->cfg.rk == 4)
     for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = state(&h->b.K_bulk[i], &h->b.K_B[i]);
   if (e == cudaSuccess) e = dalloc(h, &h->b.PA, 8 * cs * tsz);
-  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+  for (int d = 0; d < 3 && e == cudaSuccess && !lean(h); ++d) {
     if (d < nd) e = dalloc(h, &h->b.F[d], 8 * cs * tsz);
     else h->b.F[d] = h->b.F[0];
   }
+  if (e == cudaSuccess && lean(h)) e = dalloc(h, &h->b.Bf, 6 * cs * tsz);
   // CTU-Hancock: predicted primitives of each direction
   for (int d = 0; d < 3 && e == cudaSuccess && h->cfg.godunov == MGPU_GODUNOV_PLM_MUSCL; ++d) {
     if (d < nd) e = dalloc(h, &h->b.Pd[d], 8 * cs * tsz);
@@ -394,13 +404,21 @@ int mgpu_num_zones(const mgpu_solver *h, long long *nz)
   return MGPU_OK;
 }
 
-static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_out, int kind)
+static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_out, int kind, long long zbeg = 0,
+                    long long zcount = -1)
 {
-  // kind 0: upload committed state, 1: download committed state, 2: upload PA, 3: download PA
+  // kind 0: upload committed state, 1: download committed state, 2: upload PA, 3: download PA;
+  // zones [zbeg, zbeg + zcount) of the guarded array (all of it when zcount < 0), host[0] being
+  // zone zbeg
   int rc = ensure_ready(h);
   if (rc) return rc;
+  if (lean(h) && kind >= 2)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout keeps the committed primitives in the stage array");
   const TransferArgs t = transfer_args(h);
-  const long long nz = h->g.nz;
+  if (zcount < 0) zcount = h->g.nz - zbeg;
+  if (zbeg < 0 || zbeg + zcount > h->g.nz) return fail(h, MGPU_ERR_ARG, "zone range outside the guarded array");
+  const long long nz = zbeg + zcount;
+  host -= zbeg * 8;
   const bool upload = kind == 0 || kind == 2;
   if (dev_in || dev_out) {
     double *d = (double *) (dev_in ? const_cast<void *>(dev_in) : dev_out);
@@ -408,11 +426,12 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
     if (kind == 0) e = fp32(h) ? upload_fp32(t, d, 0, nz) : upload_fp64(t, d, 0, nz);
     else if (kind == 1) e = fp32(h) ? download_fp32(t, d, 0, nz) : download_fp64(t, d, 0, nz);
     else e = fp32(h) ? face_io_fp32(t, d, 0, nz, kind == 3) : face_io_fp64(t, d, 0, nz, kind == 3);
+    (void) host;
     CK(e);
     CK(cudaStreamSynchronize(h->stream));
     return MGPU_OK;
   }
-  for (long long z0 = 0; z0 < nz; z0 += h->staging_zones) {
+  for (long long z0 = zbeg; z0 < nz; z0 += h->staging_zones) {
     const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
     const size_t bytes = (size_t) cnt * 8 * sizeof(double);
     if (upload) {
@@ -454,6 +473,16 @@ int mgpu_download_prim_device(mgpu_solver *h, void *dev_aos)
   if (!dev_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
   return transfer(h, nullptr, nullptr, dev_aos, 1);
 }
+int mgpu_upload_prim_range(mgpu_solver *h, const double *host_aos, long long z0, long long count)
+{
+  if (!host_aos || count < 0) return fail(h, MGPU_ERR_ARG, "bad primitive range");
+  return transfer(h, const_cast<double *>(host_aos), nullptr, nullptr, 0, z0, count);
+}
+int mgpu_download_prim_range(mgpu_solver *h, double *host_aos, long long z0, long long count)
+{
+  if (!host_aos || count < 0) return fail(h, MGPU_ERR_ARG, "bad primitive range");
+  return transfer(h, host_aos, nullptr, nullptr, 1, z0, count);
+}
 int mgpu_set_primitive(mgpu_solver *h, const double *host_aos)
 {
   if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
@@ -467,6 +496,7 @@ static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
   A.pp = phys(h);
   A.rk = h->cfg.rk;
   A.godunov = h->cfg.godunov;
+  A.lean = lean(h);
   A.ereset = h->cfg.ereset;
   A.preset = h->cfg.preset;
   A.dreset = h->cfg.dreset;
@@ -623,7 +653,7 @@ int mgpu_measure_divB_state(mgpu_solver *h, double *mean, double *max)
   }
   CK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  const double *B = h->b.Pc_B[h->ctl_host->cur];
+  const double *B = lean(h) ? (h->ctl_host->cur ? h->b.U1_B : h->b.U0_B) : h->b.Pc_B[h->ctl_host->cur];
   k_divB_state<<<RED_BLOCKS, 256, 0, h->stream>>>(h->g, B, h->red);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->red_host, h->red, sizeof(double) * 2 * RED_BLOCKS, cudaMemcpyDeviceToHost, h->stream));
@@ -713,6 +743,7 @@ int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double
   A.pp = phys(h);
   A.rk = h->cfg.rk;
   A.godunov = h->cfg.godunov;
+  A.lean = lean(h);
   A.ereset = h->cfg.ereset;
   A.preset = h->cfg.preset;
   A.dreset = h->cfg.dreset;
@@ -751,6 +782,7 @@ int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult)
   if (total > 0 && !mult) return fail(h, MGPU_ERR_ARG, "external guards need multiplicity tables");
   if (total > 0 && h->cfg.godunov != MGPU_GODUNOV_PLM_SPLIT)
     return fail(h, MGPU_ERR_UNSUPPORTED, "the CTU-Hancock operator runs on single domains only");
+  if (total > 0 && lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   for (long long i = 0; i < total; ++i)
     if (mult[i] < 1) return fail(h, MGPU_ERR_ARG, "multiplicities must be >= 1");
   if (h->mult) cudaFree(h->mult);
@@ -792,6 +824,7 @@ static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pac
   if (rc) return rc;
   if (!buf || dim < 0 || dim >= h->g.nd || (which != 0 && which != 1) || (side != 0 && side != 1))
     return fail(h, MGPU_ERR_ARG, "bad halo arguments");
+  if (lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   TransferArgs t = transfer_args(h);
   if (which == 1) {
     rc = read_ctl(h);
@@ -818,6 +851,7 @@ int mgpu_internal_state(mgpu_solver *h, Grid *g, AdvanceBuffers *b, Ctl **ctl, v
 {
   int rc = ensure_ready(h);
   if (rc) return rc;
+  if (lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "pairs are harvested from standard-layout solvers");
   *g = h->g;
   *b = h->b;
   *ctl = h->ctl;

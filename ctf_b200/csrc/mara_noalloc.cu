@@ -68,7 +68,8 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   }
   if (cfg->fluid != MGPU_FLUID_RMHD || cfg->precision != MGPU_PREC_FP64 || cfg->rk < 1 || cfg->rk > 4 ||
       cfg->recon < 0 || cfg->recon > 2 || cfg->riemann < 0 || cfg->riemann > 2 || cfg->is_mode < 0 ||
-      cfg->is_mode > 2 || !(cfg->gamma > 1.0) || cfg->learned_c2p || cfg->godunov != MGPU_GODUNOV_PLM_SPLIT) {
+      cfg->is_mode > 2 || !(cfg->gamma > 1.0) || cfg->learned_c2p || cfg->godunov != MGPU_GODUNOV_PLM_SPLIT ||
+      cfg->layout != MGPU_LAYOUT_STANDARD) {
     put_err(errbuf, errbuf_len,
             "mgpu_advance_noalloc: needs an rmhd FP64 plm-split configuration without a learned c2p network");
     return MGPU_ERR_ARG;

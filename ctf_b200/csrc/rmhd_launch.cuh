@@ -8,6 +8,7 @@
 #include "rmhd_step.cuh"
 #include "rmhd_step_tc.cuh"
 #include "rmhd_ctu.cuh"
+#include "rmhd_lean.cuh"
 
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
@@ -38,9 +39,64 @@ inline void launch_flux(const Grid &g, int d, int rs, unsigned grid, unsigned bl
 // before PH_COMMIT.
 enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3 };
 
+// The phases of an advance in the lean layout (rmhd_lean.cuh): no P->U (the committed state
+// is conserved), no c2p at the first stage, sweeps that accumulate into U[!cur], CT from the
+// stored face fields, and after the commit a restore c2p that runs only if nothing committed.
+template <class T>
+inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
+{
+  const Grid &g = A.g;
+  const AdvanceBuffers &b = A.b;
+  cudaStream_t st = A.stream;
+  const StatePtr<T> UA{(T *) b.U0_bulk, b.U0_B}, UB{(T *) b.U1_bulk, b.U1_B};
+  T *PA = (T *) b.PA;
+  T *Bf = (T *) b.Bf;
+  const int ns = num_stages(A.rk);
+  LaunchProfiler *pr = A.prof;
+  const unsigned zb = 256;
+  const unsigned zgrid = (unsigned) ((g.ninterior + zb - 1) / zb);
+  const unsigned cgrid = (unsigned) ((g.ninterior + 127) / 128);
+  const StateCPtr<T> none{nullptr, nullptr};
+  auto c2p = [&](int mode, int zero_guess, bool learned) {
+    ProfScope ps(pr, st, KC_C2P, g.ninterior);
+    if (learned) {
+      const long long ntiles = (g.ninterior + 127) / 128, tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
+      k_cons_to_prim_tc<T><<<(unsigned) (ntiles < tc_max ? ntiles : tc_max), 128, tc::SMEM_BYTES, st>>>(
+          g, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset, A.preset, A.dreset);
+    } else {
+      k_cons_to_prim<T, 2><<<cgrid, 128, 0, st>>>(g, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset,
+                                                   A.preset, A.dreset);
+    }
+  };
+  const bool learned = A.pp.learned && A.pp.mlp_tc;
+  if (phase == PH_BEGIN) {
+    ProfScope ps(pr, st, KC_BEGIN, 1);
+    k_begin<<<1, 32, 0, st>>>(A.ctl, A.dt_mode, A.dt, A.cfl, A.min_dx);
+  } else if (phase == PH_C2P) {
+    if (s > 0) c2p(s == ns ? C2P_LEAN_CLOSING : C2P_LEAN_STAGE, 0, learned);
+  } else if (phase == PH_FLUX_UPDATE) {
+    const StageKind kind = stage_kind(A.rk, s);
+    const LeanCombine c = lean_combine(kind.combine);
+    for (int d = 1; d <= 3; ++d) {
+      ProfScope ps(pr, st, KC_FLUX, g.ninterior);
+      launch_lean_sweep<T>(g, d, A.pp.riemann, st, PA, UA, UB, Bf, c, A.pp, A.ctl, s);
+    }
+    ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
+    k_lean_ct<T><<<zgrid, zb, 0, st>>>(g, kind.combine, UA, UB, Bf, A.ctl, s);
+  } else if (phase == PH_COMMIT) {
+    {
+      ProfScope ps(pr, st, KC_BEGIN, 1);
+      k_commit<<<1, 32, 0, st>>>(A.ctl, ns);
+    }
+    c2p(C2P_LEAN_RESTORE, 1, false);
+  }
+  return cudaGetLastError();
+}
+
 template <class T>
 inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
 {
+  if (A.lean) return launch_lean_phase<T>(A, phase, s);
   const Grid &g = A.g;
   const AdvanceBuffers &b = A.b;
   cudaStream_t st = A.stream;
@@ -198,6 +254,12 @@ template <class T>
 inline cudaError_t launch_upload(const TransferArgs &A, const double *d_aos, long long z0, long long count)
 {
   const unsigned blk = 256, grid = (unsigned) ((count + blk - 1) / blk);
+  if (A.lean) {
+    k_lean_upload<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count, (T *) A.b.PA,
+                                                 StatePtr<T>{(T *) A.b.U0_bulk, A.b.U0_B},
+                                                 StatePtr<T>{(T *) A.b.U1_bulk, A.b.U1_B}, A.gamma, A.ctl);
+    return cudaGetLastError();
+  }
   k_aos_to_state<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count, StatePtr<T>{(T *) A.b.Pc_bulk[0], A.b.Pc_B[0]},
                                                 StatePtr<T>{(T *) A.b.Pc_bulk[1], A.b.Pc_B[1]}, A.ctl);
   return cudaGetLastError();
@@ -207,6 +269,12 @@ template <class T>
 inline cudaError_t launch_download(const TransferArgs &A, double *d_aos, long long z0, long long count)
 {
   const unsigned blk = 256, grid = (unsigned) ((count + blk - 1) / blk);
+  if (A.lean) {
+    k_lean_download<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count, (const T *) A.b.PA,
+                                                   StateCPtr<T>{(const T *) A.b.U0_bulk, A.b.U0_B},
+                                                   StateCPtr<T>{(const T *) A.b.U1_bulk, A.b.U1_B}, A.ctl);
+    return cudaGetLastError();
+  }
   k_state_to_aos<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count,
                                                 StateCPtr<T>{(const T *) A.b.Pc_bulk[0], A.b.Pc_B[0]},
                                                 StateCPtr<T>{(const T *) A.b.Pc_bulk[1], A.b.Pc_B[1]}, A.ctl);

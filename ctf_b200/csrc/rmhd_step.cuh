@@ -156,9 +156,12 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
                                            int ereset, double preset, double dreset, int i, int j, int k,
                                            const double *u, double *p, int err, const C2PTally &tally)
 {
-  warp_add(&ctl->c2p_calls, 1u);
-  warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
-  if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
+  const bool counted = final != C2P_LEAN_RESTORE;
+  if (counted) {
+    warp_add(&ctl->c2p_calls, 1u);
+    warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
+    if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
+  }
   if (err) {
     if (ereset) {   // emergency reset of the failed zone
       p[0] = dreset;
@@ -168,8 +171,9 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
       p[6] = u[6];
       p[7] = u[7];
       if (final == 2) atomicAdd(&ctl->ctu_reset, 1);
-    } else {
-      atomicAdd(final == 1 ? &ctl->final_err : final == 2 ? &ctl->ctu_c2p_err : &ctl->stage_err[stage],
+    } else if (counted) {
+      const bool closing = final == C2P_CLOSING || final == C2P_LEAN_CLOSING;
+      atomicAdd(closing ? &ctl->final_err : final == C2P_CTU_STAGE ? &ctl->ctu_c2p_err : &ctl->stage_err[stage],
                 multiplicity(g, i, j, k));
     }
   }
@@ -189,8 +193,32 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
         } else {
 #pragma unroll
           for (int q = 0; q < 8; ++q) PA[q * g.cs + w] = T(p[q]);
+          if (final == C2P_LEAN_CLOSING) {   // the field of the register about to be committed
+#pragma unroll
+            for (int q = 0; q < 3; ++q) Pn.B[q * g.cs + w] = u[5 + q];
+          }
         }
       }
+}
+
+// The conserved input of a c2p launch: U, or in the lean layout one of the two conserved
+// registers (Pn0 = U[0], Pn1 = U[1]) by the committed role bit ctl->cur -- U[cur] for the
+// restore, U[!cur] (the RK register) otherwise.
+template <class T>
+__device__ __forceinline__ StateCPtr<T> c2p_input(const Ctl *ctl, int final, StateCPtr<T> U, StatePtr<T> Pn0,
+                                                  StatePtr<T> Pn1)
+{
+  if (final < C2P_LEAN_STAGE) return U;
+  const int r = final == C2P_LEAN_RESTORE ? ctl->cur : ctl->cur ^ 1;
+  const StatePtr<T> R = r ? Pn1 : Pn0;
+  return StateCPtr<T>{R.bulk, R.B};
+}
+
+// Whether a c2p launch has nothing to do: an earlier stage failed, or (restore) the advance
+// committed.
+__device__ __forceinline__ bool c2p_skip(const Ctl *ctl, int stage, int final)
+{
+  return final == C2P_LEAN_RESTORE ? ctl->committed != 0 : stage_failed(ctl, stage);
 }
 
 // One interior zone's c2p.  Guess: 0 compiles in the per-thread network guess (used when
@@ -218,10 +246,11 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, Sta
                                                       PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
                                                       int ereset, double preset, double dreset)
 {
-  if (stage_failed(ctl, stage)) return;
+  if (c2p_skip(ctl, stage, final)) return;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.ninterior) return;
-  c2p_zone<T, Guess>(g, U, PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess, final, ereset, preset, dreset, t);
+  c2p_zone<T, Guess>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess,
+                     final, ereset, preset, dreset, t);
 }
 
 // ---- flux sweep (MethodOfLinesSplit::intercell_flux_sweep, Mara/plm-split.cpp:43-73) ---------
@@ -234,11 +263,11 @@ struct FluxTally {
   int hlld_ok, hlld_hllc, pcm_retry, face_c2p_calls, face_c2p_iters;
 };
 
-// One face: reconstruct, Riemann solve (PCM retry on failure), store the flux; the face's
-// |lambda| is folded into ml.
+// One face: reconstruct, Riemann solve (PCM retry on failure), the flux in Fo (zero when both
+// attempts fail); the face's |lambda| is folded into ml.
 template <class T, int dim, int RS>
-__device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ PA, T *__restrict__ F,
-                                          const PhysParams &pp, long long f, T &ml, FluxTally &ft)
+__device__ __forceinline__ void face_flux(const Grid &g, const T *__restrict__ PA, const PhysParams &pp, long long f,
+                                          T &ml, FluxTally &ft, T *Fo)
 {
   const long long S = g.s[dim - 1];
   T Pl[8], Pr[8];
@@ -259,7 +288,6 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
       Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
     }
   }
-  T Fo[8];
   const T gamma = T(pp.gamma);
   int err = 1, used_hllc = 0;
   constexpr bool hlld = RS == RIEMANN_HLLD;
@@ -287,14 +315,23 @@ __device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ P
 #pragma unroll
     for (int q = 0; q < 8; ++q) Fo[q] = T(0);
   }
-#pragma unroll
-  for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
   if constexpr (hlld) {
     ft.hlld_ok += 1 - used_hllc;
     ft.hlld_hllc += used_hllc;
   }
   ft.face_c2p_calls += tally.attempts > 0;
   ft.face_c2p_iters += tally.iters;
+}
+
+// One face, its flux stored in F.
+template <class T, int dim, int RS>
+__device__ __forceinline__ void flux_face(const Grid &g, const T *__restrict__ PA, T *__restrict__ F,
+                                          const PhysParams &pp, long long f, T &ml, FluxTally &ft)
+{
+  T Fo[8];
+  face_flux<T, dim, RS>(g, PA, pp, f, ml, ft, Fo);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) F[q * g.cs + f] = Fo[q];
 }
 
 // MaxLambda of a block: warp max -> block max -> one atomicMax (non-negative doubles order

@@ -22,9 +22,10 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
                                                          int zero_guess, int final, int ereset, double preset,
                                                          double dreset)
 {
-  if (stage_failed(ctl, stage)) return;
+  if (c2p_skip(ctl, stage, final)) return;
   extern __shared__ unsigned char tc_smem[];
   tc::TcNet net = tc::tc_setup(tc_smem, (const unsigned char *) pp.mlp_tc);
+  U = c2p_input(ctl, final, U, Pn0, Pn1);
   const long long ntiles = (g.ninterior + 127) / 128;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long t = tile * 128 + threadIdx.x;

@@ -35,6 +35,17 @@ struct PhysParams {
 
 constexpr int MAX_STAGES = 4;
 
+// What a c2p launch reads, where it writes and which counter its failures go to.
+enum C2PMode {
+  C2P_STAGE = 0,          // stage input -> PA, failures abort the stage
+  C2P_CLOSING = 1,        // final state -> the uncommitted primitive buffer
+  C2P_CTU_STAGE = 2,      // CTU-Hancock stage input -> PA, failures do not abort
+  // lean layout: the conserved registers are U[cur] (committed) and U[!cur] (RK register)
+  C2P_LEAN_STAGE = 3,     // U[!cur] -> PA
+  C2P_LEAN_CLOSING = 4,   // U[!cur] -> PA, plus its field to U[!cur]'s guard images
+  C2P_LEAN_RESTORE = 5    // U[cur] -> PA after an advance that did not commit; uncounted
+};
+
 // Device control block of one solver (one per handle, in device memory).
 struct Ctl {
   unsigned long long max_lambda_bits;   // MaxLambda of the current/last advance (double bits)
@@ -101,6 +112,7 @@ struct AdvanceBuffers {
   double *U0_B, *U1_B, *K_B[3];
   void *F[3];
   void *Pd[3];   // CTU-Hancock: predicted primitives per direction (8 x T each)
+  void *Bf;      // lean layout: the six transverse magnetic face fluxes (6 x T)
 };
 
 // Optional per-launch timing: the launcher records an event pair around every kernel and
@@ -139,6 +151,7 @@ struct AdvanceArgs {
   PhysParams pp;
   int rk;           // 1 single, 2 rk2, 3 rk3, 4 rk4
   int godunov;      // 0 method of lines (plm-split), 1 CTU-Hancock (plm-muscl)
+  int lean = 0;     // 1: lean layout (rmhd_lean.cuh)
   int ereset;
   double preset, dreset;
   int dt_mode;      // 0: dt from the host, 1: dt = cfl*min_dx/MaxLambda(previous)
@@ -181,6 +194,8 @@ struct TransferArgs {
   Ctl *ctl;
   cudaStream_t stream;
   int cur;   // committed buffer, for the halo copies of the committed state
+  int lean = 0;        // lean layout: the committed state is (PA, U[cur]); see rmhd_lean.cuh
+  double gamma = 0.0;  // for the lean upload's P->U
 };
 
 // One member of an ensemble of boxes (device-side descriptor).

@@ -32,6 +32,7 @@ ADVANCE = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}
 IS_MODE = {"js96": 0, "b08": 1, "sz10": 2}
 PRECISION = {"fp64": 0, "fp32": 1}
 GODUNOV = {"plm-split": 0, "plm-muscl": 1}   # method of lines / CTU-Hancock
+LAYOUT = {"standard": 0, "lean": 1}          # device memory layout (include/mara_gpu.h)
 PRIM_NAMES = ["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]   # Mara/rmhd.cpp:72-78
 
 
@@ -60,6 +61,7 @@ class Scheme:
     precision: str = "fp64"
     learned_c2p: bool = False
     godunov: str = "plm-split"   # 'plm-muscl': CTU-Hancock with PLM slopes of limiter theta
+    layout: str = "standard"     # 'lean': 144 B per zone in FP32 bulk, for 3D boxes up to 1024^3
 
     def to_config(self) -> _lib.MgpuConfig:
         lib = _lib.load()
@@ -79,6 +81,7 @@ class Scheme:
         c.precision = PRECISION[self.precision]
         c.learned_c2p = int(self.learned_c2p)
         c.godunov = GODUNOV[self.godunov]
+        c.layout = LAYOUT[self.layout]
         return c
 
 
@@ -143,6 +146,16 @@ class Solver:
             out = np.empty(self.shape)
         self._check_buf(out)
         self._check(self.lib.mgpu_download_prim(self.h, _dp(out)))
+        return out
+
+    def upload_range(self, P: np.ndarray, z0: int):
+        """Zones [z0, z0 + len) of the guarded zone order from an (m, 8) float64 array."""
+        P = np.ascontiguousarray(P, dtype=np.float64).reshape(-1, 8)
+        self._check(self.lib.mgpu_upload_prim_range(self.h, _dp(P), int(z0), P.shape[0]))
+
+    def download_range(self, z0: int, count: int) -> np.ndarray:
+        out = np.empty((int(count), 8))
+        self._check(self.lib.mgpu_download_prim_range(self.h, _dp(out), int(z0), int(count)))
         return out
 
     def upload_device(self, ptr: int):

@@ -29,6 +29,7 @@ enum { MGPU_RIEMANN_HLL = 0, MGPU_RIEMANN_HLLC = 1, MGPU_RIEMANN_HLLD = 2 };
 enum { MGPU_IS_JS96 = 0, MGPU_IS_B08 = 1, MGPU_IS_SZ10 = 2 };
 enum { MGPU_PREC_FP64 = 0, MGPU_PREC_FP32 = 1 };
 enum { MGPU_GODUNOV_PLM_SPLIT = 0, MGPU_GODUNOV_PLM_MUSCL = 1 };
+enum { MGPU_LAYOUT_STANDARD = 0, MGPU_LAYOUT_LEAN = 1 };
 #define MGPU_KERNEL_CLASSES 6
 
 /* Solver selection: the union of Mara.set_fluid/set_eos/set_godunov/set_riemann/set_advance
@@ -56,6 +57,19 @@ typedef struct {
                           limiter `theta`, PlmCtuHancockOperator, Mara/ctu-hancock.cpp:53-494;
                           single domains only: not with external guards, ensembles or
                           mgpu_advance_noalloc) */
+  int    layout;       /* device memory layout (no counterpart in the reference, whose state
+                          is host memory).  MGPU_LAYOUT_STANDARD: stored face fluxes, two
+                          committed primitive buffers (304 B per guarded zone in FP32 bulk,
+                          512 B in FP64).  MGPU_LAYOUT_LEAN: 3D boxes too large for that
+                          (a 1024^3 FP32-bulk box): the sweeps add their flux differences
+                          straight into the Runge-Kutta register and only the six transverse
+                          face fields are stored (144 B per zone in FP32 bulk, 240 B in FP64).
+                          Lean needs nd = 3, 'plm-split', rk 1-3 and a single domain; results
+                          agree with the standard layout to the bulk type's rounding, the
+                          magnetic field and its divergence stay FP64 as there; after a failed
+                          advance the primitives are the c2p of the unchanged conserved state;
+                          mgpu_set_primitive is not available (the stage array holds the
+                          committed primitives). */
 } mgpu_config;
 
 typedef struct {
@@ -95,6 +109,13 @@ int mgpu_upload_prim(mgpu_solver *h, const double *host_aos);
 int mgpu_download_prim(mgpu_solver *h, double *host_aos);
 int mgpu_upload_prim_device(mgpu_solver *h, const void *dev_aos);
 int mgpu_download_prim_device(mgpu_solver *h, void *dev_aos);
+/* The same for zones [z0, z0 + count) of the guarded AoS array (host pointer to count*8
+ * doubles), so that a box larger than host memory allows is filled or read slab by slab (no
+ * counterpart in the reference, whose Mara.init_prim fills one host buffer).  In the lean
+ * layout an upload takes the interior zones of the range and fills their periodic guard
+ * images; guard zones of the range are ignored. */
+int mgpu_upload_prim_range(mgpu_solver *h, const double *host_aos, long long z0, long long count);
+int mgpu_download_prim_range(mgpu_solver *h, double *host_aos, long long z0, long long count);
 
 /* replaces luaC_Mara_advance (Mara/mara.cpp:297-341) on the device-resident state:
  * returns in *errors the number of failed zones (state unchanged when > 0).  Synchronous. */

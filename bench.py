@@ -56,6 +56,16 @@ ENSEMBLE_WORKLOADS = {
     "kh_ensemble256_plm_hllc_rk3": dict(nboxes=256, lo=64, hi=512,
                                         scheme=dict(extrap="plm", riemann="hllc", advance="rk3")),
 }
+# large driven boxes in the lean layout (FP32 bulk + learned c2p), OU velocity forcing
+# (correlation time 1, forcing power 0.3^2 on 1 <= |k| <= 3), uniform start rho = p = 1,
+# B = (0, 0, 0.5), v = 0; the loop of the reference's driven-turbulence driver
+# (ctf-core/drvtrb.lua:480-488): advance, OU step of the field, resample every 10 steps
+DRIVEN_WORKLOADS = {
+    "drive1024_weno5_hlld_rk3": dict(n=(1024, 1024, 1024), power=0.09, k1=3, zeta=1.0, Bz=0.5,
+                                     scheme=dict(extrap="weno5", riemann="hlld", advance="rk3")),
+    "drive256_weno5_hlld_rk3": dict(n=(256, 256, 256), power=0.09, k1=3, zeta=1.0, Bz=0.5,
+                                    scheme=dict(extrap="weno5", riemann="hlld", advance="rk3")),
+}
 CFL = 0.3
 
 
@@ -361,6 +371,127 @@ def run_ensemble_bench(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_driven_bench(args, rank, world, local):
+    """A large driven box in the lean layout: FP32 bulk + learned c2p, OU driving, as the
+    reference's driven-turbulence driver runs it.  The box starts uniform and is filled slab
+    by slab (one x-plane of host memory); the timed region is K driver steps (get_timestep,
+    advance with its driving kick, OU step of the field, a resample every 10 steps), timed
+    with CUDA events on the solver's stream around the whole loop."""
+    import torch
+    from ctf_b200.mara import Scheme, Solver, new_ou_field
+    from ctf_b200.train_c2p import load as load_net
+    wl = DRIVEN_WORKLOADS[args.workload]
+    n, kw = wl["n"], wl["scheme"]
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    net_path = os.path.join(ROOT, "ctf_b200", "data", "c2p_net.npz")
+    learned = os.path.exists(net_path) and not args.no_learned
+    s = Solver(Scheme(precision="fp32", layout="lean", learned_c2p=learned, **kw), n, stream=stream.cuda_stream)
+    if learned:
+        s.set_c2p_network(load_net(net_path))
+    G = [m + 6 for m in n]
+    plane = np.zeros((G[1] * G[2], 8))
+    plane[:, 0] = 1.0
+    plane[:, 1] = 1.0
+    plane[:, 7] = wl["Bz"]
+    t_ic = time.perf_counter()
+    for i in range(G[0]):
+        s.upload_range(plane, i * G[1] * G[2])
+    s.set_driving(new_ou_field(3, wl["power"], wl["zeta"], wl["k1"], 1000 + rank))
+    t_ic = time.perf_counter() - t_ic
+    assert s.advance(0.0) == 0, "priming advance failed"
+    it = [0]
+
+    def driver_step():
+        dt = s.get_timestep(CFL)
+        e = s.advance(dt)
+        if e == 0:
+            s.driving_advance(dt)
+            if it[0] % 10 == 0:
+                s.driving_resample()
+        it[0] += 1
+        return e
+
+    for _ in range(args.warmup):
+        assert driver_step() == 0
+    s.profile_enable(capacity=64 * (args.steps + 1))
+    s.profile_read()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    errs = 0
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            errs += driver_step()
+        end.record(stream)
+        end.synchronize()
+    ms = start.elapsed_time(end)
+    prof = s.profile_read()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    zones = int(np.prod(n))
+    st = s.stats()
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    state = 5 * 4 + 3 * 8
+    # lean sweeps: read the 8 FP32 stage primitives, write two face fields, read-modify-write
+    # the 5 FP32 register components (the x sweep also reads U^n): averaged over x, y, z
+    per_unit = {"flux": 32 + 8 + (60 + 40 + 40) / 3.0,
+                "update": 3 * 8 * 3 + 6 * 4,       # CT: read U^n.B, U^(s).B, write U.B, read 6 face fields
+                "c2p": state + 8 * 4}
+    dom = max(("flux", "update", "c2p"), key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    alg = per_unit[dom] * d["units"] / max(d["launches"], 1)
+    achieved = alg / (d["ms"] / max(d["launches"], 1) * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": zones * args.steps * world / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n": list(n), "scheme": kw, "cfl": CFL, "layout": "lean",
+                   "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
+                                + ("; learned c2p guess (bf16 tcgen05 MLP)" if learned else ""),
+                   "driving": {k: wl[k] for k in ("power", "k1", "zeta")} | {"resample_every": 10},
+                   "ic": f"uniform rho=p=1, Bz={wl['Bz']}, v=0 (driven from rest), {t_ic:.0f} s to fill",
+                   "l2": "every state array > 126 MB L2 (no flush needed)",
+                   "parallelism": f"{world} independent replica(s)",
+                   "device_bytes_per_zone": 144},
+        "gpu_launches": int(sum(v["launches"] for v in prof.values())),
+        "clocks": clk.summary(), "errors": errs,
+        "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},
+        "c2p_iters_per_call": st["c2p_iters"] / max(st["c2p_calls"], 1),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes_per_unit": per_unit[dom],
+                     "kernel_share": {k: v["ms"] / sum(x["ms"] for x in prof.values()) for k, v in prof.items()}},
+        "e2e": None,
+        "e2e_note": "not measured for this workload: the AoS host buffer of a 1030^3 box is 70 GB per direction",
+    }
+    s.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, v, sec = cpu_sample(kw, steps=2, n=48)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                               "sample": f"48^3 turbulence box, same scheme (undriven), 2 steps after priming "
+                                         f"({sec:.1f} s), interior zone-updates/s on 1 core"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def run_reference_arm(args, wl_name, rank, world):
     """--impl reference: the reference's own CPU advance on every host core (independent
     replicas of a 64^3 sample box of the workload's scheme, or 256^2 KH boxes for an
@@ -388,7 +519,10 @@ def run_reference_arm(args, wl_name, rank, world):
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
-    n_wl, _, scheme_kw = WORKLOADS[wl_name]
+    if wl_name in DRIVEN_WORKLOADS:
+        n_wl, scheme_kw = DRIVEN_WORKLOADS[wl_name]["n"], DRIVEN_WORKLOADS[wl_name]["scheme"]
+    else:
+        n_wl, _, scheme_kw = WORKLOADS[wl_name]
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     n = 64 if n_wl[0] >= 64 else n_wl[0]
@@ -420,7 +554,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(ENSEMBLE_WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + sorted(ENSEMBLE_WORKLOADS) + sorted(DRIVEN_WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -437,6 +572,9 @@ def main():
         return
     if args.workload in ENSEMBLE_WORKLOADS:
         run_ensemble_bench(args, rank, world, local)
+        return
+    if args.workload in DRIVEN_WORKLOADS:
+        run_driven_bench(args, rank, world, local)
         return
 
     import torch

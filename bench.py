@@ -561,6 +561,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--layout", default="standard", choices=["standard", "lean"],
+                    help="device layout of the turbulence workloads (lean: 3D, 144 B per zone in FP32)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -607,7 +609,8 @@ def main():
     head_key = "fp32+learned" if net is not None else "fp32"
     for prec, learned in runs:
         key = prec + ("+learned" if learned else "")
-        s = Solver(Scheme(precision=prec, learned_c2p=learned, **scheme_kw), n, stream=stream.cuda_stream)
+        s = Solver(Scheme(precision=prec, learned_c2p=learned, layout=args.layout, **scheme_kw), n,
+                   stream=stream.cuda_stream)
         if learned:
             s.set_c2p_network(net)
         s.upload(P0)
@@ -644,12 +647,12 @@ def main():
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL,
+        "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL, "layout": args.layout,
                    "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
                                 + ("; learned c2p guess (bf16 tcgen05 MLP)" if head_key.endswith("learned") else ""),
                    "dt": dt_fixed, "l2": "every state array > 126 MB L2 (no flush needed)",
                    "parallelism": f"{world} independent replica(s)"},
-        "gpu_launches": launches_per_step(len(n), scheme_kw["advance"]) * args.steps,
+        "gpu_launches": int(sum(v["launches"] for v in results[head_key]["prof"].values())),
         "clocks": head["clocks"],
     }
     def c2p_it(k):
@@ -684,6 +687,12 @@ def main():
                 "update": upd,
                 "c2p": state + 8 * tsz,                 # read U, write 8 prim comps (interior)
                 "p2c": 2 * state}
+    if args.layout == "lean":
+        # a lean sweep per interior zone: read 8 stage primitives, write 2 face fields, read-modify-
+        # write 5 register components (the x sweep also reads U^n); CT reads U^n.B, U^(s).B and six
+        # face fields, writes U.B
+        per_unit["flux"] = 8 * tsz + 2 * tsz + (3 * 5 * tsz + 2 * (2 * 5 * tsz)) / 3.0
+        per_unit["update"] = 3 * 3 * 8 + 6 * tsz
     d = prof[dom]
     alg_bytes_per_launch = per_unit[dom] * d["units"] / max(d["launches"], 1)
     avg_ms = d["ms"] / max(d["launches"], 1)
@@ -692,7 +701,7 @@ def main():
     # this scheme (profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md,
     # profiles/k_update_turb160_weno5_hlld_rk3_fp32.md), scaled to this launch's units
     measured = {("flux", "hlld"): 72.8, ("update", "hlld"): 220.2}
-    tpu = measured.get((dom, scheme_kw["riemann"])) if head_key.startswith("fp32") else None
+    tpu = measured.get((dom, scheme_kw["riemann"])) if head_key.startswith("fp32") and args.layout == "standard" else None
     traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                        "frac": achieved / hbm, "traffic": traffic,

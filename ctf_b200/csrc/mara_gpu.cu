@@ -412,8 +412,9 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
   // zone zbeg
   int rc = ensure_ready(h);
   if (rc) return rc;
-  if (lean(h) && kind >= 2)
-    return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout keeps the committed primitives in the stage array");
+  // the lean layout's stage array holds the committed primitives: setting the measured array
+  // is an upload of the committed state there (Mara.advance(buf) uploads it again anyway)
+  if (lean(h) && kind >= 2) kind -= 2;
   const TransferArgs t = transfer_args(h);
   if (zcount < 0) zcount = h->g.nz - zbeg;
   if (zbeg < 0 || zbeg + zcount > h->g.nz) return fail(h, MGPU_ERR_ARG, "zone range outside the guarded array");

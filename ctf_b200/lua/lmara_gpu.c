@@ -15,8 +15,9 @@
  * the reference outside the RMHD step (other fluids and EOSs, cooling, driving, sampling,
  * images) exist in the table and raise an error naming themselves.
  *
- * Additions: config_solver accepts precision = 'fp64' | 'fp32' (the FP32-bulk path) and
- * learned_c2p = true | false; Mara.set_c2p_network(buf) takes a buffer of float32 network
+ * Additions: config_solver accepts precision = 'fp64' | 'fp32' (the FP32-bulk path),
+ * learned_c2p = true | false and layout = 'standard' | 'lean' (the device layout of large 3D
+ * boxes, include/mara_gpu.h); Mara.set_c2p_network(buf) takes a buffer of float32 network
  * parameters; Mara.gpu_stats() returns the device counters of the last advance.
  *
  * The solver is one module-level object, as the reference's is (mara.cpp:135).  Scheme
@@ -352,6 +353,16 @@ static int l_config_solver(lua_State *L)
   if (lua_isboolean(L, -1)) {
     M.cfg.learned_c2p = lua_toboolean(L, -1);
     if (!quiet) printf("[Mara] setting learned_c2p=%d\n", M.cfg.learned_c2p);
+  }
+  lua_pop(L, 1);
+
+  lua_getfield(L, 1, "layout");
+  if (lua_isstring(L, -1)) {
+    const char *key = lua_tostring(L, -1);
+    if (strcmp(key, "standard") == 0) M.cfg.layout = MGPU_LAYOUT_STANDARD;
+    else if (strcmp(key, "lean") == 0) M.cfg.layout = MGPU_LAYOUT_LEAN;
+    else luaL_error(L, "[Mara] no such layout '%s'", key);
+    if (!quiet) printf("[Mara] setting layout=%s\n", key);
   }
   lua_pop(L, 1);
 

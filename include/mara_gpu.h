@@ -68,8 +68,8 @@ typedef struct {
                           agree with the standard layout to the bulk type's rounding, the
                           magnetic field and its divergence stay FP64 as there; after a failed
                           advance the primitives are the c2p of the unchanged conserved state;
-                          mgpu_set_primitive is not available (the stage array holds the
-                          committed primitives). */
+                          the stage array holds the committed primitives, so
+                          mgpu_set_primitive uploads the committed state. */
 } mgpu_config;
 
 typedef struct {

@@ -151,12 +151,23 @@ def test_lean_range_transfers():
     assert np.array_equal(whole[..., 5:], P0[..., 5:])
 
 
+def test_lean_set_primitive_uploads_the_committed_state():
+    """The stage array holds the committed primitives, so set_primitive (what Mara.init_prim
+    ends with) uploads them: the measures read them and the next advance starts from them."""
+    n = (8, 8, 8)
+    P0 = ics.turbulence_box(n, seed=2)
+    a, b = Solver(Scheme(layout="lean"), n), Solver(Scheme(layout="lean"), n)
+    a.set_primitive(P0.copy())
+    b.upload(P0.copy())
+    assert np.array_equal(a.download(), b.download())
+    assert a.max_lorentz_factor() == b.max_lorentz_factor()
+    assert a.advance(0.0) == 0 and b.advance(0.0) == 0
+    assert np.array_equal(a.download(), b.download())
+
+
 def test_lean_rejections():
     with pytest.raises(MaraError):
         Solver(Scheme(layout="lean"), (16, 16))                      # 3D only
-    s = Solver(Scheme(layout="lean"), (8, 8, 8))
-    with pytest.raises(MaraError):
-        s.set_primitive(np.zeros(s.shape))                          # PA holds the committed state
     with pytest.raises(MaraError):
         Solver(Scheme(layout="lean", godunov="plm-muscl"), (8, 8, 8))
     with pytest.raises(MaraError):

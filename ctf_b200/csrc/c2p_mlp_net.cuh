@@ -34,6 +34,28 @@ __device__ __forceinline__ void c2p_features(double D, double Tau, double S2, do
   x[4] = (float) (BS2 / (S2 * B2 + 1e-30));
 }
 
+// The same features and guess with FP32 transcendentals, for inference: the network reads its
+// inputs as BF16 and its guess only seeds the FP64 Newton polish, so FP32 logarithms and
+// exponentials (a few instructions each, against software FP64 routines) lose nothing.
+__device__ __forceinline__ void c2p_features_f32(double D, double Tau, double S2, double B2, double BS2, float *x)
+{
+  const double iD = 1.0 / D;
+  x[0] = log1pf((float) (Tau * iD));
+  x[1] = log1pf((float) (S2 * iD * iD));
+  x[2] = log1pf((float) (B2 * iD));
+  x[3] = log1pf((float) (BS2 * iD * iD * iD));
+  x[4] = (float) (BS2 / (S2 * B2 + 1e-30));
+}
+
+__device__ __forceinline__ bool c2p_guess_from_output_f32(double D, const float *y, double &Z, double &W)
+{
+  const float lw = y[0], lh = y[1];
+  if (!(lw >= 0.f && lw < 30.f && lh >= 0.f && lh < 60.f)) return false;
+  W = (double) expf(lw);
+  Z = D * (double) expf(lw + lh);
+  return Z > 0.0 && W >= 1.0;
+}
+
 // Per-thread forward pass in FP32 (weights read through the read-only cache).
 __device__ __forceinline__ void mlp_forward_thread(const float *__restrict__ p, const float *xin, float *y)
 {

@@ -26,9 +26,6 @@
 #pragma once
 #include "rmhd_step.cuh"
 
-#ifndef MGPU_LEAN_CHUNK
-#define MGPU_LEAN_CHUNK 32   // zones per thread of the x and y marching sweeps
-#endif
 
 namespace mgpu {
 
@@ -85,14 +82,15 @@ __device__ __forceinline__ void lean_accumulate(const Grid &g, StatePtr<T> U0, S
 
 // ---- x and y sweeps: one thread per (column, chunk), marching along the sweep direction ---------
 // Columns cover the two other dimensions with one zone of halo ([ng-1, ng+n] each: flux-CT
-// reads transverse neighbours' face fields); a chunk is MGPU_LEAN_CHUNK zones of the sweep
-// direction.  The thread computes the lower face of its first zone, then per zone the upper
+// reads transverse neighbours' face fields); a chunk is `chunk` zones of the sweep direction
+// (lean_chunk picks it per launch).  The thread computes the lower face of its first zone, then per zone the upper
 // face, and adds the difference to the zone when the column is interior.  Consecutive threads
 // take consecutive k, so every load and store is coalesced.
 template <class T, int dim, int RS>
 __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, const T *__restrict__ PA, StatePtr<T> UA,
                                                                     StatePtr<T> UB, T *__restrict__ Bf,
-                                                                    LeanCombine c, PhysParams pp, Ctl *ctl, int stage)
+                                                                    LeanCombine c, PhysParams pp, Ctl *ctl, int stage,
+                                                                    int chunk_len)
 {
   static_assert(dim == 1 || dim == 2, "x or y sweep");
   if (stage_failed(ctl, stage + 1)) return;
@@ -102,7 +100,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
   const int oa = dim == 1 ? 1 : 0;                  // the other two dimensions: a (outer), k (inner)
   const int na = g.n[oa] + 2, nk = g.n[2] + 2;
   const long long ncol = (long long) na * nk;
-  const int nchunk = (g.n[d] + MGPU_LEAN_CHUNK - 1) / MGPU_LEAN_CHUNK;
+  const int nchunk = (g.n[d] + chunk_len - 1) / chunk_len;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
@@ -115,8 +113,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
     const bool interior = a >= 1 && a <= g.n[oa] && b >= 1 && b <= g.n[2];
     const long long S = g.s[d];
     const long long base = (long long) ca * g.s[oa] + k;   // zone (0 along dim, ca, k)
-    const int m0 = g.ng + chunk * MGPU_LEAN_CHUNK;
-    const int m1 = min(m0 + MGPU_LEAN_CHUNK, g.ng + g.n[d]);
+    const int m0 = g.ng + chunk * chunk_len;
+    const int m1 = min(m0 + chunk_len, g.ng + g.n[d]);
     const T inv_dx = T(1.0 / (dim == 1 ? g.dx : g.dy));
     const T dt = T(ctl->dt);
     T *slot0 = Bf + (long long) bf_slot(dim, dim == 1 ? By : Bx) * g.cs;
@@ -291,6 +289,27 @@ __global__ void k_lean_download(Grid g, double *__restrict__ aos, long long z0, 
 }
 
 // ---- launch sequence ---------------------------------------------------------------------------
+// Chunk length of a marching sweep over ncol columns of n zones: every chunk costs one face
+// more than its zones, and the launch takes ceil(threads / resident threads) waves of
+// chunk + 1 faces each, so pick the length in [16, 64] that minimises their product.
+inline int lean_chunk(long long ncol, int n, long long resident_threads)
+{
+  int best = 32;
+  double best_cost = 1e300;
+  for (int L = 16; L <= 64; ++L) {
+    const long long nchunk = (n + L - 1) / L;
+    const long long Lr = (n + nchunk - 1) / nchunk;   // the longest chunk with this count
+    if (Lr != L) continue;
+    const long long threads = ncol * nchunk;
+    const double cost = (double) ((threads + resident_threads - 1) / resident_threads) * (double) (L + 1);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = L;
+    }
+  }
+  return best;
+}
+
 template <class T>
 inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, const T *PA, StatePtr<T> UA,
                               StatePtr<T> UB, T *Bf, const LeanCombine &c, const PhysParams &pp, Ctl *ctl, int s)
@@ -307,10 +326,11 @@ inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, c
   }
   const int oa = dim == 1 ? 1 : 0;
   const long long ncol = (long long) (g.n[oa] + 2) * (g.n[2] + 2);
-  const long long nchunk = (g.n[dim - 1] + MGPU_LEAN_CHUNK - 1) / MGPU_LEAN_CHUNK;
+  const int L = lean_chunk(ncol, g.n[dim - 1], 148ll * MGPU_FLUX_MINB * blk);
+  const long long nchunk = (g.n[dim - 1] + L - 1) / L;
   const unsigned grid = (unsigned) ((ncol * nchunk + blk - 1) / blk);
 #define MGPU_LEAN_CASE(D, R) \
-  if (dim == D && rs == R) { k_lean_sweep<T, D, R><<<grid, blk, 0, st>>>(g, PA, UA, UB, Bf, c, pp, ctl, s); return; }
+  if (dim == D && rs == R) { k_lean_sweep<T, D, R><<<grid, blk, 0, st>>>(g, PA, UA, UB, Bf, c, pp, ctl, s, L); return; }
   MGPU_LEAN_CASE(1, RIEMANN_HLLD) MGPU_LEAN_CASE(2, RIEMANN_HLLD)
   MGPU_LEAN_CASE(1, RIEMANN_HLLC) MGPU_LEAN_CASE(2, RIEMANN_HLLC)
   MGPU_LEAN_CASE(1, RIEMANN_HLL) MGPU_LEAN_CASE(2, RIEMANN_HLL)

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
         const double B2 = u[Bx] * u[Bx] + u[By] * u[By] + u[Bz] * u[Bz];
         const double BS = u[Bx] * u[Sx] + u[By] * u[Sy] + u[Bz] * u[Sz];
         float x[5];
-        c2p_features(u[ddd], u[tau], S2, B2, BS * BS, x);
+        c2p_features_f32(u[ddd], u[tau], S2, B2, BS * BS, x);
         net.normalise(x, xn);
         good = isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]) && isfinite(xn[3]) && isfinite(xn[4]);
         if (!good) xn[0] = xn[1] = xn[2] = xn[3] = xn[4] = 0.f;
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
     const bool have = net.forward(xn, y);
     if (!valid) continue;
     double Zg = 0.0, Wg = 0.0;
-    const bool use = have && good && c2p_guess_from_output(u[ddd], y, Zg, Wg);
+    const bool use = have && good && c2p_guess_from_output_f32(u[ddd], y, Zg, Wg);
     C2PTally tally;
     const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
     c2p_finish<T>(g, PA, ctl->cur ? Pn0 : Pn1, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err,

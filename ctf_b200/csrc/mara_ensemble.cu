@@ -615,14 +615,15 @@ int mgpu_ensemble_get_stats(mgpu_ensemble *e, int box, mgpu_stats *s)
   s->dt = c.dt;
   s->errors = errors_of(c, e->cfg.rk);
   s->committed = c.committed;
-  s->c2p_calls = c.c2p_calls;
-  s->c2p_iters = c.c2p_iters;
-  for (int a = 0; a < 6; ++a) s->c2p_attempt[a] = c.c2p_attempt[a];
-  s->face_c2p_calls = c.face_c2p_calls;
-  s->face_c2p_iters = c.face_c2p_iters;
-  s->hlld_ok = c.hlld_ok;
-  s->hlld_hllc = c.hlld_hllc;
-  s->pcm_retry = c.pcm_retry;
+  const StatSlot t = stat_sum(c);
+  s->c2p_calls = t.c2p_calls;
+  s->c2p_iters = t.c2p_iters;
+  for (int a = 0; a < 6; ++a) s->c2p_attempt[a] = t.c2p_attempt[a];
+  s->face_c2p_calls = t.face_c2p_calls;
+  s->face_c2p_iters = t.face_c2p_iters;
+  s->hlld_ok = t.hlld_ok;
+  s->hlld_hllc = t.hlld_hllc;
+  s->pcm_retry = t.pcm_retry;
   return MGPU_OK;
 }
 

@@ -223,8 +223,8 @@ __global__ void __launch_bounds__(128) k_ctu_predict(Grid g, StateCPtr<T> U, con
   }
   warp_add_int(&ctl->ctu_err[1], bad);
   warp_add_int(&ctl->ctu_err[2], c2p_bad);
-  warp_add(&ctl->c2p_calls, calls);
-  warp_add(&ctl->c2p_iters, iters);
+  warp_add(&stat_slot(ctl).c2p_calls, calls);
+  warp_add(&stat_slot(ctl).c2p_iters, iters);
 }
 
 static __global__ void k_ctu_close(Ctl *ctl, int stage)

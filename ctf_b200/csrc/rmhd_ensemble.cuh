@@ -46,10 +46,7 @@ static __global__ void k_ens_begin(const BoxDev *boxes, int nb, int dt_mode, con
   for (int s = 0; s < MAX_STAGES; ++s) ctl->stage_err[s] = 0;
   ctl->final_err = 0;
   ctl->committed = 0;
-  ctl->c2p_calls = ctl->c2p_iters = 0;
-  for (int a = 0; a < 6; ++a) ctl->c2p_attempt[a] = 0;
-  ctl->face_c2p_calls = ctl->face_c2p_iters = 0;
-  ctl->hlld_ok = ctl->hlld_hllc = ctl->pcm_retry = 0;
+  for (int i = 0; i < STAT_SLOTS; ++i) ctl->stat[i] = StatSlot{};
 }
 
 static __global__ void k_ens_commit(const BoxDev *boxes, int nb, int nstages, int commit)

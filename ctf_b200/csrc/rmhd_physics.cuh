@@ -1086,16 +1086,90 @@ __device__ __forceinline__ int hlld_reconstruct(const HlldEqn<T> &q, T p, T *F)
   return 0;
 }
 
+// First attempt of the HLL-state c2p in the FP32-bulk HLLD: the Anton et al. 2-D Newton of
+// c2p_anton2dzw_fast in FP32 from the average face state (in P), to a step tolerance of 1e-6,
+// with the reference's clamps, reconstruction, pressure floor and checks.  The HLL state's
+// primitives only seed the eq. 48 pressure guess and are kept in FP32 anyway, so an FP32
+// polish loses nothing; returns nonzero (the caller then runs the FP64 ladder) when the state
+// fails check_cons, the guess is unusable, Newton does not converge in 32 iterations or the
+// primitives fail check_prim.
+__device__ __forceinline__ int c2p_hll_f32(const PhysParams &pp, const float *U, float *P, int &iters)
+{
+  iters = 0;
+  if (check_cons(U)) return 1;
+  const float V2g = P[vx] * P[vx] + P[vy] * P[vy] + P[vz] * P[vz];
+  if (!(V2g < 1.f && P[rho] > 0.f && P[pre] > 0.f)) return 1;
+  const float gamma = float(pp.gamma), gamf = (gamma - 1.f) / gamma;
+  const float D = U[ddd], Tau = U[tau];
+  const float S2 = U[Sx] * U[Sx] + U[Sy] * U[Sy] + U[Sz] * U[Sz];
+  const float B2 = U[Bx] * U[Bx] + U[By] * U[By] + U[Bz] * U[Bz];
+  const float BS = U[Bx] * U[Sx] + U[By] * U[Sy] + U[Bz] * U[Sz];
+  const float BS2 = BS * BS;
+  const float W2g = 1.f / (1.f - V2g);
+  float Z = P[rho] * (1.f + P[pre] / P[rho] * (1.f / (gamma - 1.f) + 1.f)) * W2g;
+  float W = sqrtf(W2g);
+  const float iD = 1.f / D;
+  float iW = 1.f / W, iZ = 1.f / Z;
+  float error = 1.f;
+  while (error > 1e-6f) {
+    const float W2 = W * W, Z2 = Z * Z, Z3 = Z * Z2;
+    const float iW2 = iW * iW, iW3 = iW2 * iW, iZ2 = iZ * iZ, iZ3 = iZ2 * iZ;
+    const float Pre = D * iW * (Z * iD * iW - 1.f) * gamf;
+    const float BZ = B2 + Z;
+    const float df0dZ = 2.f * BZ * (BS2 * W2 + (W2 - 1.f) * Z3) * iW2 * iZ3;
+    const float df0dW = 2.f * BZ * BZ * iW3;
+    const float df1dZ = 1.f + BS2 * iZ3 - gamf * iW2;
+    const float df1dW = (B2 + (2.f * Z - D * W) * gamf) * iW3;
+    const float f0 = -S2 + BZ * BZ * (W2 - 1.f) * iW2 - (2.f * Z + B2) * BS2 * iZ2;
+    const float f1 = -Tau + Z + B2 - Pre - 0.5f * B2 * iW2 - 0.5f * BS2 * iZ2 - D;
+    const float idet = 1.f / (df0dZ * df1dW - df0dW * df1dZ);
+    const float dZ = -(df1dW * f0 - df0dW * f1) * idet;
+    const float dW = -(df0dZ * f1 - df1dZ * f0) * idet;
+    float Zn = fabsf(Z + dZ), Wn = W + dW;
+    Zn = (Zn < 1e20f) ? Zn : Z;
+    Wn = fminf(fmaxf(Wn, 1.f), 1e12f);
+    Z = Zn;
+    W = Wn;
+    iZ = 1.f / Z;
+    iW = 1.f / W;
+    error = fabsf(dZ * iZ) + fabsf(dW * iW);
+    if (!(error == error) || ++iters == 32) return 1;
+  }
+  float Q[8];
+  const float b0 = BS * W * iZ;
+  Q[rho] = D * iW;
+  Q[pre] = D * iW * (Z * iD * iW - 1.f) * gamf;
+  const float iZB = 1.f / (Z + B2);
+  Q[vx] = (U[Sx] + b0 * U[Bx] * iW) * iZB;
+  Q[vy] = (U[Sy] + b0 * U[By] * iW) * iZB;
+  Q[vz] = (U[Sz] + b0 * U[Bz] * iW) * iZB;
+  Q[Bx] = U[Bx];
+  Q[By] = U[By];
+  Q[Bz] = U[Bz];
+  if (pp.pfloor > 0.0 && Q[pre] < float(pp.pfloor)) Q[pre] = float(pp.pfloor);
+  if (check_prim(Q)) return 1;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) P[i] = Q[i];
+  return 0;
+}
+
 // Converts a flux-solver state to double for the FP64 c2p and back.  P holds the average of
 // the two face states on entry.  The FP64 path runs the reference's ladder as it is (first
-// attempt from the estimate of the conserved state).  The FP32-bulk path starts Newton from
-// the average state instead -- in smooth flow the HLL state's primitives are close to it, so
-// the polish takes 2 iterations instead of 6 (measured, 256^3 turbulence) -- and falls back to
-// the estimate and the reference ladder when that attempt fails; the root it lands on is the
-// same to the Newton tolerance.
+// attempt from the estimate of the conserved state).  The FP32-bulk path first tries
+// c2p_hll_f32; when that fails it runs the FP64 Newton from the average state -- in smooth
+// flow the HLL state's primitives are close to it, so that polish takes 2 iterations instead
+// of 6 (measured, 256^3 turbulence) -- and then the estimate and the reference ladder; the
+// root it lands on is the same to the Newton tolerance.
 template <class T>
 __device__ __forceinline__ int cons_to_prim_T(const PhysParams &pp, const T *U, T *P, C2PTally *tally)
 {
+  if constexpr (sizeof(T) < sizeof(double)) {
+    int it = 0;
+    if (c2p_hll_f32(pp, U, P, it) == 0) {
+      if (tally) { tally->iters = it; tally->attempts = 1; }
+      return 0;
+    }
+  }
   double Ud[8], Pd[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) { Ud[i] = double(U[i]); Pd[i] = double(P[i]); }

@@ -75,6 +75,16 @@ __device__ __forceinline__ void load_state(const Grid &g, StateCPtr<T> s, long l
   for (int c = 0; c < 3; ++c) U[5 + c] = s.B[c * g.cs + z];
 }
 
+// The statistics slot of the calling block.
+__device__ __forceinline__ StatSlot &stat_slot(Ctl *ctl) { return ctl->stat[blockIdx.x % STAT_SLOTS]; }
+
+// Zeroes the statistics slots (all threads of the calling block take part).
+__device__ __forceinline__ void stat_reset(Ctl *ctl)
+{
+  for (int i = threadIdx.x; i < STAT_SLOTS * (int) (sizeof(StatSlot) / 8); i += blockDim.x)
+    reinterpret_cast<unsigned long long *>(ctl->stat)[i] = 0ull;
+}
+
 // Warp-aggregated counter increment.
 __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned v)
 {
@@ -97,11 +107,8 @@ static __global__ void k_begin(Ctl *ctl, int dt_mode, double dt, double cfl, dou
     for (int s = 0; s < 4; ++s) ctl->ctu_err[s] = 0;
     ctl->ctu_c2p_err = ctl->ctu_reset = 0;
     ctl->committed = 0;
-    ctl->c2p_calls = ctl->c2p_iters = 0;
-    for (int a = 0; a < 6; ++a) ctl->c2p_attempt[a] = 0;
-    ctl->face_c2p_calls = ctl->face_c2p_iters = 0;
-    ctl->hlld_ok = ctl->hlld_hllc = ctl->pcm_retry = 0;
   }
+  if (blockIdx.x == 0) stat_reset(ctl);
 }
 
 static __global__ void k_commit(Ctl *ctl, int nstages)
@@ -158,9 +165,10 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
 {
   const bool counted = final != C2P_LEAN_RESTORE;
   if (counted) {
-    warp_add(&ctl->c2p_calls, 1u);
-    warp_add(&ctl->c2p_iters, (unsigned) tally.iters);
-    if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&ctl->c2p_attempt[tally.attempts], 1u);
+    StatSlot &st = stat_slot(ctl);
+    warp_add(&st.c2p_calls, 1u);
+    warp_add(&st.c2p_iters, (unsigned) tally.iters);
+    if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&st.c2p_attempt[tally.attempts], 1u);
   }
   if (err) {
     if (ereset) {   // emergency reset of the failed zone
@@ -351,13 +359,14 @@ __device__ __forceinline__ void flux_block_finish(double m, const FluxTally &ft,
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     if (lane == 0 && m > 0.0) atomicMax(&ctl->max_lambda_bits, (unsigned long long) __double_as_longlong(m));
   }
+  StatSlot &st = stat_slot(ctl);
   if (hlld) {
-    warp_add(&ctl->hlld_ok, (unsigned) ft.hlld_ok);
-    warp_add(&ctl->hlld_hllc, (unsigned) ft.hlld_hllc);
+    warp_add(&st.hlld_ok, (unsigned) ft.hlld_ok);
+    warp_add(&st.hlld_hllc, (unsigned) ft.hlld_hllc);
   }
-  warp_add(&ctl->pcm_retry, (unsigned) ft.pcm_retry);
-  warp_add(&ctl->face_c2p_calls, (unsigned) ft.face_c2p_calls);
-  warp_add(&ctl->face_c2p_iters, (unsigned) ft.face_c2p_iters);
+  warp_add(&st.pcm_retry, (unsigned) ft.pcm_retry);
+  warp_add(&st.face_c2p_calls, (unsigned) ft.face_c2p_calls);
+  warp_add(&st.face_c2p_iters, (unsigned) ft.face_c2p_iters);
 }
 
 template <class T, int dim, int RS>

@@ -35,6 +35,17 @@ struct PhysParams {
 
 constexpr int MAX_STAGES = 4;
 
+// Statistics counters of an advance, kept in STAT_SLOTS copies 128 bytes apart: block b adds
+// to slot b % STAT_SLOTS and the host sums the slots.  With one copy every warp's atomic went
+// to the same cache line and they serialised (2 ms per 256^3 step in the zone c2p alone).
+constexpr int STAT_SLOTS = 32;
+struct StatSlot {
+  unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
+  unsigned long long face_c2p_calls, face_c2p_iters;
+  unsigned long long hlld_ok, hlld_hllc, pcm_retry;
+  unsigned long long pad[3];   // 128 bytes
+};
+
 // What a c2p launch reads, where it writes and which counter its failures go to.
 enum C2PMode {
   C2P_STAGE = 0,          // stage input -> PA, failures abort the stage
@@ -62,10 +73,26 @@ struct Ctl {
   int ctu_c2p_err;
   int ctu_reset;
   // statistics, accumulated over the advance
-  unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
-  unsigned long long face_c2p_calls, face_c2p_iters;
-  unsigned long long hlld_ok, hlld_hllc, pcm_retry;
+  StatSlot stat[STAT_SLOTS];
 };
+
+// The statistics of an advance: the sum of the slots (host side, after a copy of the block).
+inline StatSlot stat_sum(const Ctl &c)
+{
+  StatSlot t{};
+  for (int i = 0; i < STAT_SLOTS; ++i) {
+    const StatSlot &s = c.stat[i];
+    t.c2p_calls += s.c2p_calls;
+    t.c2p_iters += s.c2p_iters;
+    for (int a = 0; a < 6; ++a) t.c2p_attempt[a] += s.c2p_attempt[a];
+    t.face_c2p_calls += s.face_c2p_calls;
+    t.face_c2p_iters += s.face_c2p_iters;
+    t.hlld_ok += s.hlld_ok;
+    t.hlld_hllc += s.hlld_hllc;
+    t.pcm_retry += s.pcm_retry;
+  }
+  return t;
+}
 
 struct Grid {
   int nd, ng;

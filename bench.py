@@ -11,6 +11,11 @@ flux-CT, CFL 0.3.  `value` is the FP32-bulk path (FP64 c2p polish, magnetic fiel
 the plain FP64 path runs the same steps in the same call and is reported beside it, with the
 relative L1 difference of every primitive between the two after the timed steps.
 
+The FP32 runs use the lean device layout by default (`--layout lean`: the sweeps add their
+flux differences straight into the Runge-Kutta register, only the transverse face fields are
+stored; `--layout standard` for the stored-flux layout); the FP64 run is the plain path in the
+standard layout, the one held to the reference's golden steps.
+
 Both precisions advance with the same fixed dt (CFL 0.3 of the primed MaxLambda) so their
 final states are comparable.  Every array (1.2 GB per FP64 state at 256^3) is larger than
 the 126 MB L2, so no flush is needed between steps.  For N > 1 (torchrun) every rank
@@ -561,8 +566,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--layout", default="standard", choices=["standard", "lean"],
-                    help="device layout of the turbulence workloads (lean: 3D, 144 B per zone in FP32)")
+    ap.add_argument("--layout", default="lean", choices=["standard", "lean"],
+                    help="device layout of the FP32 runs of the turbulence workloads (lean: 3D, 144 B per "
+                         "zone in FP32; the FP64 run always uses the standard layout)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -609,7 +615,8 @@ def main():
     head_key = "fp32+learned" if net is not None else "fp32"
     for prec, learned in runs:
         key = prec + ("+learned" if learned else "")
-        s = Solver(Scheme(precision=prec, learned_c2p=learned, layout=args.layout, **scheme_kw), n,
+        layout = args.layout if prec == "fp32" else "standard"
+        s = Solver(Scheme(precision=prec, learned_c2p=learned, layout=layout, **scheme_kw), n,
                    stream=stream.cuda_stream)
         if learned:
             s.set_c2p_network(net)
@@ -647,7 +654,8 @@ def main():
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL, "layout": args.layout,
+        "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL,
+                   "layout": f"{args.layout} (FP32 runs); standard (FP64 run)",
                    "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
                                 + ("; learned c2p guess (bf16 tcgen05 MLP)" if head_key.endswith("learned") else ""),
                    "dt": dt_fixed, "l2": "every state array > 126 MB L2 (no flush needed)",
@@ -700,7 +708,7 @@ def main():
     # DRAM bytes per work unit from one ncu capture of the same kernel on the 160^3 box of
     # this scheme (profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md,
     # profiles/k_update_turb160_weno5_hlld_rk3_fp32.md), scaled to this launch's units
-    measured = {("flux", "hlld"): 72.8, ("update", "hlld"): 220.2}
+    measured = {("flux", "hlld"): 80.0, ("update", "hlld"): 219.8}
     tpu = measured.get((dom, scheme_kw["riemann"])) if head_key.startswith("fp32") and args.layout == "standard" else None
     traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -708,8 +708,11 @@ def main():
     # DRAM bytes per work unit from one ncu capture of the same kernel on the 160^3 box of
     # this scheme (profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md,
     # profiles/k_update_turb160_weno5_hlld_rk3_fp32.md), scaled to this launch's units
-    measured = {("flux", "hlld"): 80.0, ("update", "hlld"): 219.8}
-    tpu = measured.get((dom, scheme_kw["riemann"])) if head_key.startswith("fp32") and args.layout == "standard" else None
+    # (profiles/k_lean_sweep_turb160_weno5_hlld_rk3_fp32.md for the lean sweeps: DRAM bytes per
+    # interior zone, the mean of the x, y and z sweeps)
+    measured = {("flux", "hlld", "standard"): 80.0, ("update", "hlld", "standard"): 219.8,
+                ("flux", "hlld", "lean"): 107.7}
+    tpu = measured.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
     traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                        "frac": achieved / hbm, "traffic": traffic,

@@ -341,6 +341,31 @@ __device__ __forceinline__ int c2p_reconstruct(const C2PState &s, double Z, doub
   return C2P_SUCCESS;
 }
 
+// The same reconstruction for the FP32-bulk path's Newton (c2p_anton2dzw_fast), from the
+// reciprocals of W, Z and D it holds already: one FP64 division instead of nine.  Same
+// formulas and checks; the primitives differ from c2p_reconstruct's at FP64 round-off.
+__device__ __forceinline__ int c2p_reconstruct_fast(const C2PState &s, double Z, double W, double iZ, double iW,
+                                                    double iD, double *Pout)
+{
+  double P[8];
+  const double b0 = s.BS * W * iZ;
+  const double iZB = 1.0 / (Z + s.B2);
+  P[rho] = s.D * iW;
+  P[pre] = P[rho] * (Z * iD * iW - 1.0) * s.gamf;
+  P[vx] = (s.Sxyz[0] + b0 * s.Bxyz[0] * iW) * iZB;
+  P[vy] = (s.Sxyz[1] + b0 * s.Bxyz[1] * iW) * iZB;
+  P[vz] = (s.Sxyz[2] + b0 * s.Bxyz[2] * iW) * iZB;
+  P[Bx] = s.Bxyz[0];
+  P[By] = s.Bxyz[1];
+  P[Bz] = s.Bxyz[2];
+  if (P[pre] < s.pfloor && s.pfloor > 0.0) P[pre] = s.pfloor;
+  const int e = check_prim(P);
+  if (e) return e;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) Pout[i] = P[i];
+  return C2P_SUCCESS;
+}
+
 // Anton et al. (2006) eqs 84-85, 2-D Newton in (Z, W) (Mara/rmhd-c2p.c:232-303).
 __device__ __forceinline__ int c2p_anton2dzw(const C2PState &s, double Z, double W, double *P, int &iters)
 {
@@ -410,7 +435,7 @@ __device__ __forceinline__ int c2p_anton2dzw_fast(const C2PState &s, double Z, d
     error = fabs(dZ * iZ) + fabs(dW * iW);
     if (++iters == 250) return C2P_MAXITER;
   }
-  return c2p_reconstruct(s, Z, W, P);
+  return c2p_reconstruct_fast(s, Z, W, iZ, iW, iD, P);
 }
 
 // Noble et al. (2006) 1-D Newton in Z (Mara/rmhd-c2p.c:311-376).

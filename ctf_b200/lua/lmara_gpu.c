@@ -18,7 +18,9 @@
  * Additions: config_solver accepts precision = 'fp64' | 'fp32' (the FP32-bulk path),
  * learned_c2p = true | false and layout = 'standard' | 'lean' (the device layout of large 3D
  * boxes, include/mara_gpu.h); Mara.set_c2p_network(buf) takes a buffer of float32 network
- * parameters; Mara.gpu_stats() returns the device counters of the last advance.
+ * parameters; Mara.gpu_stats() returns the device counters of the last advance;
+ * Mara.upload_primitive(buf), Mara.advance_device(dt) and Mara.download_primitive(buf) step a
+ * device-resident state without the per-step host copies of Mara.advance(buf, dt).
  *
  * The solver is one module-level object, as the reference's is (mara.cpp:135).  Scheme
  * changes after set_domain rebuild the device solver at its next use (the state lives in
@@ -28,6 +30,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "lua.h"
 #include "lauxlib.h"
@@ -49,6 +52,7 @@ typedef struct {
   char *drive;               /* driving field carried across a solver rebuild */
   long long drive_len;
   int have_godunov;          /* set_godunov was called since start */
+  int resident;              /* the device solver holds a state from upload_primitive */
 } MaraGpu;
 
 static MaraGpu M;
@@ -82,6 +86,7 @@ static mgpu_solver *solver(lua_State *L)
     }
   }
   free_solver();
+  M.resident = 0;
   mgpu_config cfg = M.cfg;
   if (cfg.godunov == MGPU_GODUNOV_PLM_MUSCL) cfg.theta = ctu_theta;
   int rc = mgpu_create(&cfg, &M.h);
@@ -463,6 +468,52 @@ static int l_advance(lua_State *L)
   return 2;
 }
 
+/* Device-resident stepping (no counterpart in the reference, whose state lives in the caller's
+ * buffer): upload_primitive(buf) copies a primitive buffer to the device once,
+ * advance_device(dt) -> kzps, errors advances it there without host copies (state unchanged
+ * when errors > 0, as Mara.advance), download_primitive(buf) copies it back.  A driver loop
+ * that only reads get_timestep and the measures between steps then moves no state over PCIe;
+ * a scheme change rebuilds the solver and needs a new upload. */
+static int l_upload_primitive(lua_State *L)
+{
+  double *buf = check_prim_buffer(L, 1);
+  const int rc = mgpu_upload_prim(solver(L), buf);
+  if (rc) return raise_abi(L, rc, "upload_primitive");
+  M.resident = 1;
+  return 0;
+}
+
+static double now_seconds(void)
+{
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double) t.tv_sec + 1e-9 * (double) t.tv_nsec;
+}
+
+static int l_advance_device(lua_State *L)
+{
+  const double dt = luaL_checknumber(L, 1);
+  mgpu_solver *h = solver(L);
+  if (!M.resident) return luaL_error(L, "[Mara] advance_device needs a state: call Mara.upload_primitive(P) first");
+  int errors = 0;
+  const double t0 = now_seconds();
+  const int rc = mgpu_advance(h, dt, &errors);
+  if (rc) return raise_abi(L, rc, "advance_device");
+  lua_pushnumber(L, 1e-3 * (double) M.nzones / (now_seconds() - t0));
+  lua_pushnumber(L, errors);
+  return 2;
+}
+
+static int l_download_primitive(lua_State *L)
+{
+  double *buf = check_prim_buffer(L, 1);
+  mgpu_solver *h = solver(L);
+  if (!M.resident) return luaL_error(L, "[Mara] download_primitive needs a state: call Mara.upload_primitive(P) first");
+  const int rc = mgpu_download_prim(h, buf);
+  if (rc) return raise_abi(L, rc, "download_primitive");
+  return 0;
+}
+
 static int l_get_timestep(lua_State *L)
 {
   const double cfl = luaL_checknumber(L, 1);
@@ -649,6 +700,9 @@ int luaopen_Mara(lua_State *L)
       {"new_ou_field", l_new_ou_field},
       {"set_driving", l_set_driving},
       {"gpu_stats", l_gpu_stats},
+      {"upload_primitive", l_upload_primitive},
+      {"advance_device", l_advance_device},
+      {"download_primitive", l_download_primitive},
       {NULL, NULL}};
   static const char *const absent[] = {"show", "diffuse", "set_failmask", "prim_at_point", "set_units",
                                        "set_cooling", "set_fluxsrc", "set_srcterm",

@@ -75,6 +75,9 @@ def test_module_surface_without_a_gpu():
         assert(not ok and msg:find("no such extrap 'ppm'"))
         ok, msg = pcall(Mara.advance, buffer.new_buffer(64), 0.0)
         assert(not ok and msg:find('need a domain to run this'))
+        ok, msg = pcall(Mara.advance_device, 0.0)
+        assert(not ok and msg:find('need a domain to run this'))
+        assert(type(Mara.upload_primitive) == 'function' and type(Mara.download_primitive) == 'function')
         """)
         with pytest.raises(LuaError, match="boom"):
             h.run("error('boom')")
@@ -118,3 +121,36 @@ def test_driver_script_matches_the_reference(tmp_path, kw):
     assert abs(mg[0] - mr[0]) <= 1e-9 * abs(mr[1])
     assert abs(mg[1] - mr[1]) <= 1e-9 * abs(mr[1])
     assert abs(mg[2] - mr[2]) <= 1e-12 * mr[2]
+
+
+# The same driver loop on a device-resident state: one upload, advance_device per step (no
+# host copies), one download at the end.
+RESIDENT = DRIVER.replace("local kz, e = Mara.advance(P, 0.0)",
+                          "Mara.upload_primitive(P)\nlocal kz, e = Mara.advance_device(0.0)") \
+                 .replace("kz, e = Mara.advance(P, dt)", "kz, e = Mara.advance_device(dt)") \
+                 .replace("log:close()", "log:close()\nMara.download_primitive(P)")
+
+
+@needs_host
+@pytest.mark.gpu
+def test_device_resident_loop_matches_the_reference(tmp_path):
+    """Mara.upload_primitive / advance_device / download_primitive: the reference's driver loop
+    without the per-step host round trips gives the reference's states, dt and error counts."""
+    assert RESIDENT != DRIVER and "advance_device(dt)" in RESIDENT
+    kw = dict(riemann="hlld", advance="rk2", extrap="plm")
+    n = (12, 10, 8)
+    P0 = ics.turbulence_box(n, seed=73, vrms=0.2)
+    inp = tmp_path / "P0.bin"
+    P0.astype(np.float64).tofile(inp)
+    out = tmp_path / "P_res.bin"
+    with LuaHost() as h:
+        h.run(RESIDENT.format(inp=inp, out=out, steps=4, n0=n[0], n1=n[1], n2=n[2], **kw))
+    Pg = np.fromfile(out).reshape(P0.shape)
+    lg = open(str(out) + ".txt").read().split("\n")
+    Pr, lr = _run_driver(tmp_path, "ref", kw, n, 4, P0)
+    for a, b in zip(lg[:5], lr[:5]):
+        ea, eb = a.split(), b.split()
+        assert ea[0] == eb[0]
+        if len(ea) > 1:
+            assert abs(float(ea[1]) - float(eb[1])) <= 1e-12 * float(eb[1])
+    assert np.abs(Pg - Pr).max() <= 1e-10 * np.abs(Pr).max()

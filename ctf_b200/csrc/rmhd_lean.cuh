@@ -122,6 +122,13 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
 #pragma unroll 1
     for (int m = m0 - 1; m < m1; ++m) {   // face between zones m and m + 1
       const long long f = base + (long long) m * S;
+      if (m >= m0 && interior) {   // the register entries this face updates: into L2 while HLLD runs
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(U1.bulk + q * g.cs + f));
+          if (dim == 1) asm volatile("prefetch.global.L2 [%0];" ::"l"(U0.bulk + q * g.cs + f));
+        }
+      }
       T Fo[8];
       face_flux<T, dim, RS>(g, PA, pp, f, ml, ft, Fo);
       if (m >= m0 || chunk == 0) {            // the chunk's first face is its neighbour's last
@@ -164,6 +171,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
     const int a = (int) (row / nj), b = (int) (row - (long long) a * nj);
     const int i = g.ng - 1 + a, j = g.ng - 1 + b;
     f = (long long) i * g.s[0] + (long long) j * g.s[1] + (g.ng - 1 + fk);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) asm volatile("prefetch.global.L2 [%0];" ::"l"(U1.bulk + r * g.cs + f));
     T Fo[8];
     face_flux<T, 3, RS>(g, PA, pp, f, ml, ft, Fo);
     if (threadIdx.x > 0 || blockIdx.x == 0) {

@@ -525,14 +525,20 @@ static __device__ __noinline__ C2PRungs c2p_rungs(const C2PState s, C2PRungs r)
 // follows unchanged if that attempt fails.  The first Anton attempt is inlined (one call
 // site serves both the learned and the estimated starting point); the other rungs are not.
 // Guess (compile time): 0 = the per-thread network when pp.learned; 1 = the given (Zg, Wg)
-// when `have`; 2 = none (no network code is compiled in).
-template <bool Fast = false, int Guess = 0>
+// when `have`; 2 = none (no network code is compiled in).  `prev` fills P with the previous
+// primitive state when P does not hold it yet: it is called only on the paths that read P
+// (the ladder's rungs) or leave it as the result (a failure), so a caller can defer that load.
+struct C2PPrevInP {
+  __device__ void operator()(double *) const {}
+};
+template <bool Fast = false, int Guess = 0, class Prev = C2PPrevInP>
 __device__ __forceinline__ int cons_to_prim(const PhysParams &pp, const double *U, double *P,
                                             C2PTally *tally = nullptr, double Zg = 0.0, double Wg = 0.0,
-                                            bool have = true)
+                                            bool have = true, const Prev &prev = Prev())
 {
   int error = check_cons(U);
   if (error) {
+    prev(P);
     if (tally) { tally->iters = 0; tally->attempts = 0; }
     return error;
   }
@@ -564,6 +570,7 @@ __device__ __forceinline__ int cons_to_prim(const PhysParams &pp, const double *
     if (error && a == 0) attempts = 5;
   }
   if (error) {
+    prev(P);
     C2PRungs r;
 #pragma unroll
     for (int i = 0; i < 8; ++i) r.P[i] = P[i];

@@ -242,10 +242,13 @@ __device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, S
   const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
   double u[8], p[8];
   load_state(g, U, z, u);
+  // the previous primitives are read only when the ladder needs them or a failure keeps them
+  const auto prev = [&](double *q) {
 #pragma unroll
-  for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+    for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+  };
   C2PTally tally;
-  const int err = cons_to_prim<(sizeof(T) < sizeof(double)), Guess>(pp, u, p, &tally) != 0;
+  const int err = cons_to_prim<(sizeof(T) < sizeof(double)), Guess>(pp, u, p, &tally, 0.0, 0.0, true, prev) != 0;
   c2p_finish<T>(g, PA, Pn, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err, tally);
 }
 

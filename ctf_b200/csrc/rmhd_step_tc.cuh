@@ -39,8 +39,6 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
       interior_coords(g, t, i, j, k);
       z = ((long long) i * g.G[1] + j) * g.G[2] + k;
       load_state(g, U, z, u);
-#pragma unroll
-      for (int c = 0; c < 8; ++c) p[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
       if (check_cons(u) == C2P_SUCCESS) {
         const double S2 = u[Sx] * u[Sx] + u[Sy] * u[Sy] + u[Sz] * u[Sz];
         const double B2 = u[Bx] * u[Bx] + u[By] * u[By] + u[Bz] * u[Bz];
@@ -58,7 +56,12 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
     double Zg = 0.0, Wg = 0.0;
     const bool use = have && good && c2p_guess_from_output_f32(u[ddd], y, Zg, Wg);
     C2PTally tally;
-    const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use) != 0;
+    // the previous primitives are read only when the ladder needs them or a failure keeps them
+    const auto prev = [&](double *q) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+    };
+    const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use, prev) != 0;
     c2p_finish<T>(g, PA, ctl->cur ? Pn0 : Pn1, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err,
                   tally);
   }

@@ -1,6 +1,7 @@
 """FP32-bulk (optionally + learned c2p) against the plain FP64 path over many steps.
 
     python -m ctf_b200.accuracy [--n 512] [--steps 100] [--scheme plm,hlld,rk3] [--learned]
+                                [--layout lean|standard]
 
 Both paths advance the same seeded turbulence box with the same fixed dt (CFL 0.3 of the
 FP64 path's primed MaxLambda) and are compared after every `--every` steps: relative L1 and
@@ -38,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--scheme", default="plm,hlld,rk3")
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--layout", default="lean", choices=["lean", "standard"],
+                    help="device layout of the FP32 path (the FP64 path is the standard layout)")
     args = ap.parse_args(argv)
     import torch
     from . import ics
@@ -50,7 +53,7 @@ def main(argv=None):
     ic_sec = time.time() - t0
     ref = Solver(Scheme(extrap=extrap, riemann=riemann, advance=advance), n)
     fast = Solver(Scheme(extrap=extrap, riemann=riemann, advance=advance, precision="fp32",
-                         learned_c2p=args.learned), n)
+                         learned_c2p=args.learned, layout=args.layout), n)
     if args.learned:
         from .train_c2p import load
         fast.set_c2p_network(load())
@@ -70,7 +73,8 @@ def main(argv=None):
         a, b = fast.download(), ref.download()
         l1, linf = rel_errors(a, b)
         dm, dx = fast.mean_max_divB_state()
-        print(json.dumps({"n": args.n, "scheme": args.scheme, "learned": args.learned, "step": done, "dt": dt,
+        print(json.dumps({"n": args.n, "scheme": args.scheme, "learned": args.learned, "layout": args.layout,
+                          "step": done, "dt": dt,
                           "l1_rel": l1, "linf_rel": linf, "divB_fp32": [dm, dx],
                           "failed_zones_total": errs, "ic_seconds": round(ic_sec, 1)}), flush=True)
     ref.close()

@@ -259,9 +259,8 @@ __global__ void k_drive_sample(Grid g, int nd, int k1, const double2 *modes, con
   const int numk = nd == 3 ? r * r * r : r * r;
   for (long long z = (long long) blockIdx.x * blockDim.x + threadIdx.x; z < g.nz;
        z += (long long) gridDim.x * blockDim.x) {
-    const int i = (int) (z / g.s[0]);
-    const int j = (int) ((z / g.s[1]) % g.G[1]);
-    const int k = (int) (z % g.G[2]);
+    int i, j, k;
+    zone_coords(g, z, i, j, k);
     const double2 *px = phase + (size_t) 0 * r * gmax;
     const double2 *py = phase + (size_t) 1 * r * gmax;
     const double2 *pz = phase + (size_t) 2 * r * gmax;
@@ -355,7 +354,8 @@ __global__ void k_drive_kick_lean(Grid g, int nd, const FT *F, T *PA, StatePtr<T
     PA[vy * g.cs + z] = T(p[vy]);
     PA[vz * g.cs + z] = T(p[vz]);
     PA[rho * g.cs + z] = T(p[rho]);
-    const int i = (int) (z / g.s[0]), j = (int) ((z / g.s[1]) % g.G[1]), k = (int) (z % g.G[2]);
+    int i, j, k;
+    zone_coords(g, z, i, j, k);
     if (i < g.ng || i >= g.ng + g.n[0] || j < g.ng || j >= g.ng + g.n[1] || k < g.ng || k >= g.ng + g.n[2]) continue;
 #pragma unroll
     for (int q = 0; q < 3; ++q) p[5 + q] = U.B[q * g.cs + z];

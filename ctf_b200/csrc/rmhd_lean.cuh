@@ -258,7 +258,8 @@ __global__ void k_lean_upload(Grid g, const double *__restrict__ aos, long long 
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const long long z = z0 + t;
-  const int i = (int) (z / g.s[0]), j = (int) ((z / g.s[1]) % g.G[1]), k = (int) (z % g.G[2]);
+  int i, j, k;
+  zone_coords(g, z, i, j, k);
   if (i < g.ng || i >= g.ng + g.n[0] || j < g.ng || j >= g.ng + g.n[1] || k < g.ng || k >= g.ng + g.n[2]) return;
   const StatePtr<T> U = ctl->cur ? UB : UA;
   double p[8], u[8];

@@ -119,16 +119,44 @@ template <class T> struct StateCPtr {
   const double *B;
 };
 
+// Interior flat index t -> zone coordinates (guards counted).  Indices that fit in 32 bits
+// (every box up to 1024^3: 1.1e9 guarded zones) take 32-bit unsigned division, the emulated
+// 64-bit one costing several times as many instructions; the integers are the same.
 __device__ __forceinline__ void interior_coords(const Grid &g, long long t, int &i, int &j, int &k)
 {
   const long long nyz = (long long) g.n[1] * g.n[2];
-  i = (int) (t / nyz);
-  const long long r = t - (long long) i * nyz;
-  j = (int) (r / g.n[2]);
-  k = (int) (r - (long long) j * g.n[2]);
+  if (t < (1ll << 32) && nyz < (1ll << 32)) {
+    const unsigned tt = (unsigned) t, d1 = (unsigned) nyz, d2 = (unsigned) g.n[2];
+    const unsigned ii = tt / d1, r = tt - ii * d1, jj = r / d2;
+    i = (int) ii;
+    j = (int) jj;
+    k = (int) (r - jj * d2);
+  } else {
+    i = (int) (t / nyz);
+    const long long r = t - (long long) i * nyz;
+    j = (int) (r / g.n[2]);
+    k = (int) (r - (long long) j * g.n[2]);
+  }
   i += g.ng;
   if (g.nd >= 2) j += g.ng;
   if (g.nd >= 3) k += g.ng;
+}
+
+// Guarded flat zone index z -> (i, j, k), with the same 32-bit fast path.
+__device__ __forceinline__ void zone_coords(const Grid &g, long long z, int &i, int &j, int &k)
+{
+  if (z < (1ll << 32) && g.s[0] < (1ll << 32)) {
+    const unsigned zz = (unsigned) z, s0 = (unsigned) g.s[0], G2 = (unsigned) g.G[2];
+    const unsigned ii = zz / s0, r = zz - ii * s0, jj = r / G2;
+    i = (int) ii;
+    j = (int) jj;
+    k = (int) (r - jj * G2);
+  } else {
+    i = (int) (z / g.s[0]);
+    const long long r = z - (long long) i * g.s[0];
+    j = (int) (r / g.G[2]);
+    k = (int) (r - (long long) j * g.G[2]);
+  }
 }
 
 struct AdvanceBuffers {

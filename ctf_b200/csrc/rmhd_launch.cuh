@@ -13,6 +13,33 @@
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
 #endif
+#ifndef MGPU_TC_SPLIT
+#define MGPU_TC_SPLIT 1   // learned c2p as network kernel + polish kernel (0: one fused kernel)
+#endif
+
+namespace mgpu {
+// The learned c2p: the split network + polish kernels with the guesses in `scratch` (a face
+// array, idle while the c2p runs), or the fused kernel.
+template <class T>
+inline void launch_learned_c2p(const Grid &g, cudaStream_t st, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
+                               StatePtr<T> Pn1, const PhysParams &pp, Ctl *ctl, int s, int zero_guess, int mode,
+                               int ereset, double preset, double dreset, void *scratch)
+{
+  const long long ntiles = (g.ninterior + 127) / 128;
+  if (MGPU_TC_SPLIT) {
+    const long long nmax = 148ll * MGPU_TCNET_CTAS_PER_SM;
+    float2 *guess = (float2 *) scratch;
+    k_c2p_guess_tc<T><<<(unsigned) (ntiles < nmax ? ntiles : nmax), 128, tc::SMEM_BYTES, st>>>(g, U, Pn0, Pn1, pp,
+                                                                                               ctl, s, mode, guess);
+    k_cons_to_prim_guessed<T><<<(unsigned) ntiles, 128, 0, st>>>(g, U, PA, Pn0, Pn1, pp, ctl, s, zero_guess, mode,
+                                                               ereset, preset, dreset, guess);
+  } else {
+    const long long tmax = 148ll * MGPU_TC_CTAS_PER_SM;
+    k_cons_to_prim_tc<T><<<(unsigned) (ntiles < tmax ? ntiles : tmax), 128, tc::SMEM_BYTES, st>>>(
+        g, U, PA, Pn0, Pn1, pp, ctl, s, zero_guess, mode, ereset, preset, dreset);
+  }
+}
+}  // namespace mgpu
 
 namespace mgpu {
 
@@ -60,9 +87,8 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
   auto c2p = [&](int mode, int zero_guess, bool learned) {
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
     if (learned) {
-      const long long ntiles = (g.ninterior + 127) / 128, tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
-      k_cons_to_prim_tc<T><<<(unsigned) (ntiles < tc_max ? ntiles : tc_max), 128, tc::SMEM_BYTES, st>>>(
-          g, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset, A.preset, A.dreset);
+      launch_learned_c2p<T>(g, st, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset, A.preset,
+                            A.dreset, b.Bf);
     } else {
       k_cons_to_prim<T, 2><<<cgrid, 128, 0, st>>>(g, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset,
                                                    A.preset, A.dreset);
@@ -82,7 +108,8 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
       launch_lean_sweep<T>(g, d, A.pp.riemann, st, PA, UA, UB, Bf, c, A.pp, A.ctl, s);
     }
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
-    k_lean_ct<T><<<zgrid, zb, 0, st>>>(g, kind.combine, UA, UB, Bf, A.ctl, s);
+    k_lean_ct<T><<<zgrid, zb, 0, st>>>(g, kind.combine, UA, UB, Bf, A.ctl, s,
+                                       make_double3(1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz));
   } else if (phase == PH_COMMIT) {
     {
       ProfScope ps(pr, st, KC_BEGIN, 1);
@@ -129,17 +156,13 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     const int final = s == ns ? 1 : A.godunov ? 2 : 0;
     const StateCPtr<T> Uin = (s == 0 || final == 1) ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B};
     const int zero_guess = s == 0;
-    // learned guess on the tensor cores: persistent c2p kernel, MGPU_TC_CTAS_PER_SM CTAs per SM
-    // (4 x 128 threads x 128 registers fill the register file)
+    // learned guess on the tensor cores (launch_learned_c2p; its guesses go to F[0], idle here)
     const bool tc_c2p = A.pp.learned && A.pp.mlp_tc;
     const bool simt_net = A.pp.learned && A.pp.mlp && !A.pp.mlp_tc;   // per-thread network guess
-    const long long ntiles = (g.ninterior + 127) / 128;
-    const long long tc_max = 148ll * MGPU_TC_CTAS_PER_SM;
-    const unsigned tcgrid = (unsigned) (ntiles < tc_max ? ntiles : tc_max);
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
     if (tc_c2p)
-      k_cons_to_prim_tc<T><<<tcgrid, 128, tc::SMEM_BYTES, st>>>(g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess,
-                                                                final, A.ereset, A.preset, A.dreset);
+      launch_learned_c2p<T>(g, st, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset,
+                            A.dreset, b.F[0]);
     else if (simt_net)
       k_cons_to_prim<T, 0><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
           g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);

@@ -207,7 +207,7 @@ __device__ __forceinline__ double lean_emf(const T *F, const T *G, long long z, 
 template <class T>
 __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int combine, StatePtr<T> UA, StatePtr<T> UB,
                                                                    const T *__restrict__ Bf, const Ctl *ctl,
-                                                                   int stage)
+                                                                   int stage, double3 inv)
 {
   if (stage_failed(ctl, stage + 1)) return;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,9 +225,10 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int c
   const double FzBx0 = lean_emf(zBx, xBz, z, sz, sx), FzBxm = lean_emf(zBx, xBz, z - sz, sz, sx);
   const double FxBz0 = lean_emf(xBz, zBx, z, sx, sz), FxBzm = lean_emf(xBz, zBx, z - sx, sx, sz);
   double Lb[3];
-  Lb[0] = -(0.0 - 0.0) / g.dx - (FyBx0 - FyBxm) / g.dy - (FzBx0 - FzBxm) / g.dz;
-  Lb[1] = -(FxBy0 - FxBym) / g.dx - (0.0 - 0.0) / g.dy - (FzBy0 - FzBym) / g.dz;
-  Lb[2] = -(FxBz0 - FxBzm) / g.dx - (FyBz0 - FyBzm) / g.dy - (0.0 - 0.0) / g.dz;
+  // the zeroed normal fluxes drop out; 1/dx from the host instead of six FP64 divisions
+  Lb[0] = -(FyBx0 - FyBxm) * inv.y - (FzBx0 - FzBxm) * inv.z;
+  Lb[1] = -(FxBy0 - FxBym) * inv.x - (FzBy0 - FzBym) * inv.z;
+  Lb[2] = -(FxBz0 - FxBzm) * inv.x - (FyBz0 - FyBzm) * inv.y;
   const double dtd = ctl->dt;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {

@@ -473,9 +473,16 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
     // CT2d: Fx[Bx] = 0, Fx[By] = FxBy, Fy[Bx] = FyBx, Fy[By] = 0; Bz keeps its Godunov fluxes
     const double FxBy0 = ct_emf(F, G, g, By, Bx, z, sx, sy), FxBym = ct_emf(F, G, g, By, Bx, z - sx, sx, sy);
     const double FyBx0 = ct_emf(G, F, g, Bx, By, z, sy, sx), FyBxm = ct_emf(G, F, g, Bx, By, z - sy, sy, sx);
-    Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy;
-    Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy;
-    Lb[2] = -(fval(F, g, Bz, z) - fval(F, g, Bz, z - sx)) / dx - (fval(G, g, Bz, z) - fval(G, g, Bz, z - sy)) / dy;
+    if constexpr (sizeof(T) < sizeof(double)) {   // FP32 bulk: reciprocals, zeroed fluxes dropped
+      const double idx = 1.0 / dx, idy = 1.0 / dy;
+      Lb[0] = -(FyBx0 - FyBxm) * idy;
+      Lb[1] = -(FxBy0 - FxBym) * idx;
+      Lb[2] = -(fval(F, g, Bz, z) - fval(F, g, Bz, z - sx)) * idx - (fval(G, g, Bz, z) - fval(G, g, Bz, z - sy)) * idy;
+    } else {   // the reference's expressions, bit for bit
+      Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy;
+      Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy;
+      Lb[2] = -(fval(F, g, Bz, z) - fval(F, g, Bz, z - sx)) / dx - (fval(G, g, Bz, z) - fval(G, g, Bz, z - sy)) / dy;
+    }
   } else {
     const double FxBy0 = ct_emf(F, G, g, By, Bx, z, sx, sy), FxBym = ct_emf(F, G, g, By, Bx, z - sx, sx, sy);
     const double FyBx0 = ct_emf(G, F, g, Bx, By, z, sy, sx), FyBxm = ct_emf(G, F, g, Bx, By, z - sy, sy, sx);
@@ -483,9 +490,16 @@ __device__ __forceinline__ void update_zone(const Grid &g, const UpdateArgs &a, 
     const double FzBy0 = ct_emf(H, G, g, By, Bz, z, sz, sy), FzBym = ct_emf(H, G, g, By, Bz, z - sz, sz, sy);
     const double FzBx0 = ct_emf(H, F, g, Bx, Bz, z, sz, sx), FzBxm = ct_emf(H, F, g, Bx, Bz, z - sz, sz, sx);
     const double FxBz0 = ct_emf(F, H, g, Bz, Bx, z, sx, sz), FxBzm = ct_emf(F, H, g, Bz, Bx, z - sx, sx, sz);
-    Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy - (FzBx0 - FzBxm) / dz;
-    Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy - (FzBy0 - FzBym) / dz;
-    Lb[2] = -(FxBz0 - FxBzm) / dx - (FyBz0 - FyBzm) / dy - (0.0 - 0.0) / dz;
+    if constexpr (sizeof(T) < sizeof(double)) {   // FP32 bulk: reciprocals, zeroed fluxes dropped
+      const double idx = 1.0 / dx, idy = 1.0 / dy, idz = 1.0 / dz;
+      Lb[0] = -(FyBx0 - FyBxm) * idy - (FzBx0 - FzBxm) * idz;
+      Lb[1] = -(FxBy0 - FxBym) * idx - (FzBy0 - FzBym) * idz;
+      Lb[2] = -(FxBz0 - FxBzm) * idx - (FyBz0 - FyBzm) * idy;
+    } else {   // the reference's expressions, bit for bit
+      Lb[0] = -(0.0 - 0.0) / dx - (FyBx0 - FyBxm) / dy - (FzBx0 - FzBxm) / dz;
+      Lb[1] = -(FxBy0 - FxBym) / dx - (0.0 - 0.0) / dy - (FzBy0 - FzBym) / dz;
+      Lb[2] = -(FxBz0 - FxBzm) / dx - (FyBz0 - FyBzm) / dy - (0.0 - 0.0) / dz;
+    }
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {

@@ -140,3 +140,27 @@ def test_learned_guess_gains_over_the_method_without_it(trained, precision):
     rel = np.abs(out[True] - out[False]).max() / np.abs(out[False]).max()
     assert rel <= (1e-9 if precision == "fp64" else 1e-5), rel
     assert its[True] < 0.8 * its[False], its
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_learned_guess_under_the_ctu_operator(trained, precision):
+    """The learned guess with the CTU-Hancock operator (plm-muscl, the driven-turbulence
+    driver's scheme), whose passes write the face array the network's guesses are kept in
+    during the c2p: two steps land on the state the plain ladder gives."""
+    params, _ = trained
+    n = (24, 20, 16)
+    P0 = ics.turbulence_box(n, seed=78, vrms=0.3)
+    out, its = {}, {}
+    for learned in (False, True):
+        s = Solver(Scheme(precision=precision, learned_c2p=learned, godunov="plm-muscl", advance="single"), n)
+        s.set_c2p_network(params)
+        s.upload(P0.copy())
+        assert s.advance(0.0) == 0
+        dt = s.get_timestep(0.24)
+        assert s.advance(dt) == 0 and s.advance(dt) == 0
+        st = s.stats()
+        its[learned] = st["c2p_iters"] / st["c2p_calls"]
+        out[learned] = s.download()
+    rel = np.abs(out[True] - out[False]).max() / np.abs(out[False]).max()
+    assert rel <= (1e-9 if precision == "fp64" else 1e-5), rel
+    assert its[True] < its[False], its

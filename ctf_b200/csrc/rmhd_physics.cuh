@@ -1053,13 +1053,6 @@ __device__ __forceinline__ int hlld_reconstruct(const HlldEqn<T> &q, T p, T *F)
   else if (lmaR < s && s <= ap) region = 4;
   else if (ap < s) region = 5;
   else region = 6;   // unordered (NaN) speeds: the reference leaves F unset
-  if (region == 0 || region == 5) {
-    const T *Fo = region == 0 ? q.Fl : q.Fr;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) F[i] = Fo[i];
-    F[tau] -= F[ddd];
-    return 0;
-  }
   if (region == 6) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) F[i] = T(0);
@@ -1069,8 +1062,29 @@ __device__ __forceinline__ int hlld_reconstruct(const HlldEqn<T> &q, T p, T *F)
   const HlldJump<T> &J = left ? q.L : q.R;
   const HlldInner<T> &a = left ? aL : aR;
   const T *Uo = left ? q.Ul : q.Ur;
-  const T *Fo = left ? q.Fl : q.Fr;
   const T wave = left ? am : ap;
+  // The outer flux.  FP32 bulk recovers it from the jump across the fast wave, Fo = wave Uo - J,
+  // so that Fl and Fr are dead through the pressure iteration (sixteen registers); FP64 keeps
+  // the stored flux.
+  T Fo[8];
+  if constexpr (sizeof(T) < sizeof(double)) {
+    Fo[ddd] = wave * Uo[ddd] - J.D;
+    Fo[tau] = wave * Uo[tau] - J.E;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      Fo[Sx + k] = wave * Uo[Sx + k] - J.m[k];
+      Fo[Bx + k] = wave * Uo[Bx + k] - J.B[k];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) Fo[i] = left ? q.Fl[i] : q.Fr[i];
+  }
+  if (region == 0 || region == 5) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) F[i] = Fo[i];
+    F[tau] -= F[ddd];
+    return 0;
+  }
   // States between the fast and Alfven waves (aL / aR)
   T aU[8];
   T denom;
@@ -1222,6 +1236,35 @@ __device__ __forceinline__ int cons_to_prim_T(const PhysParams &pp, const T *U, 
   return e;
 }
 
+// HLL total pressure, EstimateSolution(0) (riemann_hlld-rmhd.cpp:543-553), from the HLL
+// state's primitives.
+template <class T>
+__device__ __forceinline__ T hlld_estimate0(const T *P)
+{
+  const T V2 = P[vx] * P[vx] + P[vy] * P[vy] + P[vz] * P[vz];
+  const T B2 = P[Bx] * P[Bx] + P[By] * P[By] + P[Bz] * P[Bz];
+  const T Bv = P[Bx] * P[vx] + P[By] * P[vy] + P[Bz] * P[vz];
+  const T W2 = T(1) / (T(1) - V2);
+  const T W = m_sqrt(W2);
+  const T b0 = W * Bv;
+  const T b2 = (B2 + b0 * b0) / W2;
+  return P[pre] + T(0.5) * b2;
+}
+
+// Eq. (55), EstimateSolution(1) (riemann_hlld-rmhd.cpp:557-574): the smaller root of
+// p^2 + (E - Fm) p + (FE m - E Fm) = 0 from the HLL state's total energy E, normal momentum m
+// and their fluxes.
+template <class T>
+__device__ __forceinline__ T hlld_estimate1(T E, T FE, T m, T Fm)
+{
+  const T a = T(1);
+  const T b = E - Fm;
+  const T c = FE * m - E * Fm;
+  const T p1 = m_abs((-b + m_sqrt(b * b - T(4) * a * c)) / (T(2) * a));
+  const T p2 = m_abs((-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a));
+  return (p1 < p2) ? p1 : p2;
+}
+
 // HlldRmhdRiemannSolver::IntercellFlux at s = 0 (riemann_hlld-rmhd.cpp:179-313).
 // Returns 1 when a face state is unphysical (the caller retries with PCM states);
 // `used_hllc` reports the fallback.
@@ -1262,6 +1305,14 @@ __device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, c
     F_hll[i] = (ap * q.Fl[i] - am * q.Fr[i] + ap * am * (q.Ur[i] - q.Ul[i])) / (ap - am);
   }
   const int hll_c2p_failed = cons_to_prim_T(pp, U_hll, P_hll, tally);
+  // FP32 bulk takes both pressure estimates here, so that P_hll, U_hll and F_hll are dead
+  // through the pressure iteration; FP64 keeps the reference's order (and its in-place shift
+  // and restore of tau, which the Bx ~ 0 retries repeat).
+  T p_est0 = T(0), p_est1 = T(0);
+  if constexpr (sizeof(T) < sizeof(double)) {
+    p_est0 = hlld_estimate0(P_hll);
+    p_est1 = hlld_estimate1(U_hll[tau] + U_hll[ddd], F_hll[tau] + F_hll[ddd], U_hll[Sx], F_hll[Sx]);
+  }
   // HlldEquation48 constructor (riemann_hlld-rmhd.cpp:315-345)
   q.ap = ap; q.am = am; q.PlBx = Pl[Bx]; q.PrBx = Pr[Bx];
   q.Ul[tau] += q.Ul[ddd];
@@ -1285,27 +1336,16 @@ __device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, c
     T p_star;
     int rc;
     const int est = (m_abs(Pl[Bx]) < T(Tol::bx_small) || m_abs(Pr[Bx]) < T(Tol::bx_small)) ? 1 : attempt;
-    if (est == 0) {   // HLL total pressure (EstimateSolution(0))
-      const T *P = P_hll;
-      const T V2 = P[vx] * P[vx] + P[vy] * P[vy] + P[vz] * P[vz];
-      const T B2 = P[Bx] * P[Bx] + P[By] * P[By] + P[Bz] * P[Bz];
-      const T Bv = P[Bx] * P[vx] + P[By] * P[vy] + P[Bz] * P[vz];
-      const T W2 = T(1) / (T(1) - V2);
-      const T W = m_sqrt(W2);
-      const T b0 = W * Bv;
-      const T b2 = (B2 + b0 * b0) / W2;
-      p_star = P[pre] + T(0.5) * b2;
-    } else if (est == 1) {   // eq. (55) (EstimateSolution(1)), which shifts and restores tau
+    if constexpr (sizeof(T) < sizeof(double)) {
+      p_star = est == 0 ? p_est0 : (est == 1 ? p_est1 : T(0));
+    } else if (est == 0) {
+      p_star = hlld_estimate0(P_hll);
+    } else if (est == 1) {   // EstimateSolution(1) shifts tau and restores it afterwards
       F_hll[tau] += F_hll[ddd];
       U_hll[tau] += U_hll[ddd];
-      const T a = T(1);
-      const T b = U_hll[tau] - F_hll[Sx];
-      const T c = F_hll[tau] * U_hll[Sx] - U_hll[tau] * F_hll[Sx];
-      const T p1 = m_abs((-b + m_sqrt(b * b - T(4) * a * c)) / (T(2) * a));
-      const T p2 = m_abs((-b - m_sqrt(b * b - T(4) * a * c)) / (T(2) * a));
+      p_star = hlld_estimate1(U_hll[tau], F_hll[tau], U_hll[Sx], F_hll[Sx]);
       F_hll[tau] -= F_hll[ddd];
       U_hll[tau] -= U_hll[ddd];
-      p_star = (p1 < p2) ? p1 : p2;
     } else {
       p_star = T(0);
     }

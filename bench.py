@@ -711,7 +711,7 @@ def main():
     # (profiles/k_lean_sweep_turb160_weno5_hlld_rk3_fp32.md for the lean sweeps: DRAM bytes per
     # interior zone, the mean of the x, y and z sweeps)
     measured = {("flux", "hlld", "standard"): 80.0, ("update", "hlld", "standard"): 219.8,
-                ("flux", "hlld", "lean"): 108.3}
+                ("flux", "hlld", "lean"): 105.1}
     tpu = measured.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
     traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -26,7 +26,7 @@ namespace mgpu {
 
 // Tolerances of the Riemann solvers.  For double they are the reference's literals; the
 // float set is scaled to FP32 resolution (the FP32 bulk path has no reference oracle and is
-// judged against the FP64 path).
+// compared with the FP64 path).
 template <class T> struct RmhdTol;
 template <> struct RmhdTol<double> {
   static constexpr double newton_eps = 1e-12;   // NewtonRaphesonSolver(15, 1e-12)
@@ -400,7 +400,7 @@ __device__ __forceinline__ int c2p_anton2dzw(const C2PState &s, double Z, double
 
 // The same Anton et al. Newton iteration with the divisions replaced by three reciprocals
 // per iteration (1/W, 1/Z, 1/det); algebraically identical, rounded differently.  Used by
-// the FP32-bulk path, whose c2p is an FP64 polish judged against the FP64 path rather than
+// the FP32-bulk path, whose c2p is an FP64 polish compared with the FP64 path rather than
 // the reference's bit pattern.
 __device__ __forceinline__ int c2p_anton2dzw_fast(const C2PState &s, double Z, double W, double *P, int &iters)
 {

@@ -14,7 +14,7 @@ from ctf_b200.mara import Scheme, Solver
 
 pytestmark = pytest.mark.gpu
 
-L1_TOL = 1e-5          # relative L1 per field (north-star density bound, applied to every field)
+L1_TOL = 1e-5          # relative L1 per field (the FP32 density target, applied to every field)
 LINF_TOL = 5e-3        # relative L-infinity per field (FP32 rounding at discontinuities)
 DIVB_TOL = 1e-12       # corner divergence of B (as Mara.measure.mean_max_divB reports it)
 
@@ -65,7 +65,7 @@ def run(prec, kw, n, P0, dt, steps):
 # amplifies the FP32 rounding of the face states (not of the solver: FP64 star-state
 # arithmetic from the same FP32 states gives the same errors).  On the 3D turbulence boxes
 # this leaves 5e-4 in the transverse velocities after 6 steps (density 9e-6), so that case
-# carries HLLC_L1_TOL; the 2D KH boxes (config 3, uniform normal field on x faces) stay at
+# carries HLLC_L1_TOL; the 2D KH boxes of the ensemble workload (uniform normal field on x faces) stay at
 # 1e-6 (test_fp32_bulk_kelvin_helmholtz_2d).  HLLD has no such division.
 HLLC_L1_TOL = 1e-3
 
@@ -88,7 +88,7 @@ def test_fp32_bulk_tracks_fp64_turbulence(kw, n, steps, vrms, l1_tol):
     a = run("fp32", kw, n, P0, dt, steps)
     b = run("fp64", kw, n, P0, dt, steps)
     l1, linf = rel_errors(a.download(), b.download(), 3)
-    assert l1[0] <= L1_TOL, l1            # density: the north-star bound, every case
+    assert l1[0] <= L1_TOL, l1            # density: the FP32 target, every case
     assert l1.max() <= l1_tol, l1
     if l1_tol == L1_TOL:                  # HLLC: a few weak-normal-field zones differ by O(0.1)
         assert linf.max() <= LINF_TOL, linf

@@ -81,7 +81,7 @@ def test_lean_failure_restores_the_state(golden):
 
 @pytest.mark.parametrize("learned", [False, True])
 def test_lean_fp32_tracks_fp64(learned):
-    """FP32 bulk in the lean layout against the plain FP64 path: the north-star L1 bound,
+    """FP32 bulk in the lean layout against the plain FP64 path: the FP32 L1 target,
     the FP32 L-infinity bound, and flux-CT's weighted divergence held to round-off."""
     from ctf_b200 import train_c2p
     n = (32, 32, 32)

@@ -18,7 +18,7 @@ from oracle import PortOracle, Scheme as OracleScheme
 
 pytestmark = pytest.mark.gpu
 
-STEP_TOL = 1e-10        # relative L-infinity per primitive component
+STEP_TOL = 1e-10        # relative L-infinity per primitive component (the FP64 parity target after 20 steps)
 DT_TOL = 1e-12          # relative, dt and MaxLambda
 # Fixtures whose reference result is itself ill-conditioned in libm: the 2D KH layer has
 # nearly double roots in the fast-speed quartic, and tests/test_oracle_port.py measures

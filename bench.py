@@ -720,6 +720,16 @@ def main():
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
                        "algorithmic_bytes_per_unit": per_unit[dom]}
+    # What bounds the FP32 HLLD sweeps instead of HBM: instruction issue and latency of the
+    # ~10^3-operation face (ncu figures of the same kernels on the 160^3 box of this scheme)
+    limiter = {("flux", "hlld", "lean"): {"issue_active": 0.467, "fma_pipe": 0.281, "xu_pipe": 0.194,
+                                          "dram_throughput": 0.068,
+                                          "source": "profiles/k_lean_sweep_turb160_weno5_hlld_rk3_fp32.md"},
+               ("flux", "hlld", "standard"): {"issue_active": 0.500, "fma_pipe": 0.292, "xu_pipe": 0.210,
+                                              "source": "profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md"}}
+    lim = limiter.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
+    if lim:
+        out["roofline"]["limiter"] = {"kind": "instruction issue / latency (FP32 pipes)", **lim}
     # every kernel class against the HBM roofline (algorithmic bytes / event-timed duration)
     out["kernels"] = {}
     for k in ("flux", "update", "c2p", "p2c"):

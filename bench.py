@@ -176,8 +176,9 @@ def rel_l1(a, b, nd, ng=3):
     return out
 
 
-def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0):
-    """Time the reference's CPU advance (or the C restatement) on a bounded sample box."""
+def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0, warmup=0):
+    """Time the reference's CPU advance (or the C restatement) on a bounded sample box, after
+    `warmup` untimed advances."""
     from oracle import PortOracle, REF_SO, RefOracle, Scheme
     sch = Scheme(n=(n, n, n), **scheme_kw)
     kind = "reference" if (use_ref and os.path.exists(REF_SO)) else "port"
@@ -185,6 +186,8 @@ def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0):
     P = make_ic("turbulence", (n, n, n), seed=seed)
     o.advance(P, 0.0)
     dt = o.get_timestep(CFL)
+    for _ in range(warmup):
+        o.advance(P, dt)
     t0 = time.perf_counter()
     for _ in range(steps):
         o.advance(P, dt)
@@ -195,12 +198,13 @@ def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0):
 
 
 def _cpu_worker(args):
-    scheme_kw, steps, n, seed = args
-    return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed)
+    scheme_kw, steps, n, seed, warmup = args
+    return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed, warmup=warmup)
 
 
-def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0):
-    """The reference's CPU advance of one 2D Kelvin-Helmholtz box (bounded sample)."""
+def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0, warmup=0):
+    """The reference's CPU advance of one 2D Kelvin-Helmholtz box (bounded sample), after
+    `warmup` untimed advances."""
     from ctf_b200 import ics
     from oracle import PortOracle, REF_SO, RefOracle, Scheme
     sch = Scheme(n=(n, n), **scheme_kw)
@@ -209,6 +213,8 @@ def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0):
     P = np.ascontiguousarray(ics.kh_box((n, n), seed=seed))
     o.advance(P, 0.0)
     dt = o.get_timestep(CFL)
+    for _ in range(warmup):
+        o.advance(P, dt)
     t0 = time.perf_counter()
     for _ in range(steps):
         o.advance(P, dt)
@@ -219,8 +225,8 @@ def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0):
 
 
 def _cpu_worker_kh(args):
-    scheme_kw, steps, n, seed = args
-    return cpu_sample_kh(scheme_kw, steps=steps, n=n, seed=seed)
+    scheme_kw, steps, n, seed, warmup = args
+    return cpu_sample_kh(scheme_kw, steps=steps, n=n, seed=seed, warmup=warmup)
 
 
 def run_ensemble_bench(args, rank, world, local):
@@ -510,7 +516,7 @@ def run_reference_arm(args, wl_name, rank, world):
         ctx = mp.get_context("spawn")
         t0 = time.perf_counter()
         with ctx.Pool(cores) as pool:
-            res = pool.map(_cpu_worker_kh, [(kw, args.steps, 256, s) for s in range(cores)])
+            res = pool.map(_cpu_worker_kh, [(kw, args.steps, 256, s, args.warmup) for s in range(cores)])
         wall = time.perf_counter() - t0
         value = float(sum(r[1] for r in res))
         line = {"metric": "RMHD zone-updates/s on 1 B200: ensemble of 256 uneven 2D KH boxes, FP32 bulk, "
@@ -535,7 +541,7 @@ def run_reference_arm(args, wl_name, rank, world):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s) for s in range(cores)])
+        res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s, args.warmup) for s in range(cores)])
     wall = time.perf_counter() - t0
     kind = res[0][0]
     value = float(sum(r[1] for r in res))

@@ -736,6 +736,16 @@ def main():
     lim = limiter.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
     if lim:
         out["roofline"]["limiter"] = {"kind": "instruction issue / latency (FP32 pipes)", **lim}
+    # The whole step against HBM: the compulsory state-vector transfers of one zone-update
+    # (single 2, RK2 5, RK3 8: each stage reads its register(s) and writes one) times the bytes
+    # of a state vector (64 B FP64; 44 B FP32 bulk with the FP64 field), at the headline rate
+    # of one GPU.
+    transfers = {"single": 2, "rk2": 5, "rk3": 8}.get(scheme_kw["advance"])
+    if transfers:
+        bpz = transfers * (44 if head_key.startswith("fp32") else 64)
+        step_gbs = out["value"] / world * bpz / 1e9
+        out["step_roofline"] = {"bytes_per_zone_update": bpz, "achieved": step_gbs, "peak": hbm,
+                                "unit": "GB/s", "frac": step_gbs / hbm}
     # every kernel class against the HBM roofline (algorithmic bytes / event-timed duration)
     out["kernels"] = {}
     for k in ("flux", "update", "c2p", "p2c"):

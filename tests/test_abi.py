@@ -54,6 +54,38 @@ def test_bad_config_is_rejected_without_a_gpu():
     assert not h.value
 
 
+@pytest.mark.parametrize("field,value,code", [
+    ("layout", 7, 1),                 # no such layout: MGPU_ERR_ARG
+    ("godunov", 4, 1),                # no such integration scheme
+    ("precision", 3, 1),
+    ("riemann", 3, 1),
+    ("recon", -1, 1),
+    ("gamma", 1.0, 1),                # gamma-law index must exceed 1
+])
+def test_config_fields_are_checked_without_a_gpu(field, value, code):
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    setattr(c, field, value)
+    h = ctypes.c_void_p()
+    assert lib.mgpu_create(ctypes.byref(c), ctypes.byref(h)) == code
+    assert not h.value
+
+
+@pytest.mark.parametrize("field,value", [("rk", 4), ("godunov", 1)])
+def test_lean_layout_limits_are_checked_without_a_gpu(field, value):
+    """The lean layout runs 'plm-split' with single, rk2 or rk3: other schemes are
+    MGPU_ERR_UNSUPPORTED before any device work."""
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    c.layout = 1                      # MGPU_LAYOUT_LEAN
+    setattr(c, field, value)
+    h = ctypes.c_void_p()
+    assert lib.mgpu_create(ctypes.byref(c), ctypes.byref(h)) == 5
+    assert not h.value
+
+
 def test_null_handle_is_an_argument_error():
     lib = _lib.load()
     assert lib.mgpu_advance(None, 0.0, None) == 1

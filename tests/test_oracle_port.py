@@ -132,3 +132,29 @@ def test_reference_conditioning_under_one_ulp_libm(golden, case):
     worst = _worst_step_diff(PortOracle(Scheme(**kw), perturbed_libm=True), g)
     lo, hi = LIBM_SENSITIVITY.get(case, (0.0, 1e-12))
     assert lo <= worst <= hi, worst
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(__import__("oracle").REF_SO),
+                    reason="the compiled reference (oracle/_ref) is not built")
+@pytest.mark.parametrize("IS", ["b08", "sz10"])
+def test_whole_step_weno5_smoothness_indicators_against_the_compiled_reference(IS):
+    """WENO5 with the B08 and SZ10 smoothness indicators over whole RK3 steps of a non-cubic
+    turbulence box: the restatement and the compiled reference agree bit for bit, dt chain and
+    MaxLambda included."""
+    from ctf_b200 import ics
+    from oracle import RefOracle
+    n = (10, 8, 6)
+    kw = dict(n=n, extrap="weno5", riemann="hlld", advance="rk3", IS=IS)
+    P0 = ics.turbulence_box(n, seed=11, vrms=0.3)
+    ref, port = RefOracle(Scheme(**kw)), PortOracle(Scheme(**kw))
+    try:
+        A, B = P0.copy(), P0.copy()
+        assert ref.advance(A, 0.0) == port.advance(B, 0.0) == 0
+        for _ in range(3):
+            dt = ref.get_timestep(0.3)
+            assert port.get_timestep(0.3) == dt
+            assert ref.advance(A, dt) == port.advance(B, dt) == 0
+            assert ref.max_lambda == port.max_lambda
+            assert np.array_equal(A, B)
+    finally:
+        ref.close()

@@ -4,20 +4,23 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
 
 A step is one full Mara advance (all RK stages) of a seeded synthetic box.  The headline
-workload is the 256^3 relativistic-MHD turbulence box (rho = p = 1, Gamma 4/3, Gaussian
+workload is the 512^3 relativistic-MHD turbulence box (rho = p = 1, Gamma 4/3, Gaussian
 random velocity with per-mode power ~ |k|^-2 on 1 <= |k| <= 4, rms 0.3c, |v| < 0.9;
-B = (0, 0, 1) + solenoidal perturbation of rms 0.1) with component-wise WENO5 + HLLD + RK3 +
-flux-CT, CFL 0.3.  `value` is the FP32-bulk path (FP64 c2p polish, magnetic field and dt);
-the plain FP64 path runs the same steps in the same call and is reported beside it, with the
-relative L1 difference of every primitive between the two after the timed steps.
+B = (0, 0, 1) + solenoidal perturbation of rms 0.1) with PLM (minmod theta 2) + HLLD + RK3 +
+flux-CT, CFL 0.3.  `value` is the FP32-bulk path with the learned c2p guess (FP64 c2p
+polish, magnetic field and dt); the plain FP64 path runs the same steps in the same call and
+is reported beside it -- both the parity build (every multiply and add rounded separately,
+as the reference's x86-64 build does) and the same kernels compiled with fused multiply-add
+-- with the relative L1 and Linf difference of every primitive against FP64 after the timed
+steps, and the failed zones of the timed steps.
 
 The FP32 runs use the lean device layout by default (`--layout lean`: the sweeps add their
 flux differences straight into the Runge-Kutta register, only the transverse face fields are
-stored; `--layout standard` for the stored-flux layout); the FP64 run is the plain path in the
-standard layout, the one held to the reference's golden steps.
+stored; `--layout standard` for the stored-flux layout); the FP64 runs use the standard
+layout, the one held to the reference's golden steps.
 
-Both precisions advance with the same fixed dt (CFL 0.3 of the primed MaxLambda) so their
-final states are comparable.  Every array (1.2 GB per FP64 state at 256^3) is larger than
+All precisions advance with the same fixed dt (CFL 0.3 of the primed MaxLambda) so their
+final states are comparable.  Every array (8.9 GB per FP64 state at 512^3) is larger than
 the 126 MB L2, so no flush is needed between steps.  For N > 1 (torchrun) every rank
 advances its own box: independent replicas, weak scaling, no collective on the data path.
 """
@@ -55,7 +58,7 @@ WORKLOADS = {
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
     "stress512_plm_hlld_rk3": ((512, 512, 512), "stress", dict(extrap="plm", riemann="hlld", advance="rk3")),
 }
-DEFAULT_WORKLOAD = "turb256_weno5_hlld_rk3"
+DEFAULT_WORKLOAD = "turb512_plm_hlld_rk3"
 # ensembles: 256 independent 2D Kelvin-Helmholtz boxes, sides log-uniform in 64..512
 ENSEMBLE_WORKLOADS = {
     "kh_ensemble256_plm_hllc_rk3": dict(nboxes=256, lo=64, hi=512,
@@ -72,6 +75,18 @@ DRIVEN_WORKLOADS = {
                                     scheme=dict(extrap="weno5", riemann="hlld", advance="rk3")),
 }
 CFL = 0.3
+
+# Figures from ncu captures of the FP32-bulk kernels on a 160^3 box of the same scheme,
+# keyed by (kernel class, reconstruction, Riemann solver, layout): DRAM bytes
+# (dram__bytes_read.sum + dram__bytes_write.sum) per work unit, and the issue/pipe
+# utilisation that bounds the lean HLLD sweeps.  They come from separate captures, not from
+# the run that prints them.
+NCU_TRAFFIC_PER_UNIT = {}
+NCU_LIMITER = {
+    ("flux", "weno5", "hlld", "lean"): {"issue_active": 0.467, "fma_pipe": 0.281, "xu_pipe": 0.194,
+                                        "dram_throughput": 0.068},
+    ("flux", "weno5", "hlld", "standard"): {"issue_active": 0.500, "fma_pipe": 0.292, "xu_pipe": 0.210},
+}
 
 
 def make_ic(kind, n, seed=0):
@@ -149,9 +164,12 @@ class ClockSampler:
 
 
 def time_device(solver, steps, warmup, dt, torch, stream):
-    """Warm up, then time `steps` advances with CUDA events on the solver's stream."""
+    """Warm up, then time `steps` advances with CUDA events on the solver's stream.  Returns
+    the milliseconds, the per-class kernel profile of the timed advances and the solver's
+    statistics after the warm-up (its cumulative advance counters mark the timed region)."""
     solver.advance_async(warmup, dt=dt)
     solver.synchronize()
+    st_warm = solver.stats()
     solver.profile_read()   # drop warm-up launches
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -162,7 +180,29 @@ def time_device(solver, steps, warmup, dt, torch, stream):
     end.synchronize()
     ms = start.elapsed_time(end)
     prof = solver.profile_read()
-    return ms, prof
+    return ms, prof, st_warm
+
+
+def rel_linf(a, b, nd, ng=3):
+    """max |a - b| / max |b| per primitive over the interior zones."""
+    sl = tuple(slice(ng, -ng) if d < nd else slice(None) for d in range(3))
+    a, b = a[sl], b[sl]
+    out = {}
+    for q, name in enumerate(["rho", "pre", "vx", "vy", "vz", "Bx", "By", "Bz"]):
+        den = np.abs(b[..., q]).max()
+        num = np.abs(a[..., q] - b[..., q]).max()
+        out[name] = float(num / den) if den > 0 else float(num)
+    return out
+
+
+def ghost_factor(n_sample, n_workload, ng=3):
+    """The reference advances every guarded zone (c2p over all of them, fluxes over almost
+    all faces), so its interior zone-updates/s on a small sample box understate its rate on a
+    large box by the ratio of the two boxes' guarded-to-interior zone counts."""
+    def over(m):
+        m = [m] * 3 if np.isscalar(m) else list(m)
+        return float(np.prod([(v + 2 * ng) / v for v in m]))
+    return over(n_sample) / over(n_workload)
 
 
 def rel_l1(a, b, nd, ng=3):
@@ -493,9 +533,13 @@ def run_driven_bench(args, rank, world, local):
     s.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, v, sec = cpu_sample(kw, steps=2, n=48)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+        corr = ghost_factor(48, n)
+        out["cpu_baseline"] = {"value": v * corr, "unit": UNIT, "cores": 1, "kind": kind,
+                               "measured_value": v, "ghost_correction": corr,
                                "sample": f"48^3 turbulence box, same scheme (undriven), 2 steps after priming "
-                                         f"({sec:.1f} s), interior zone-updates/s on 1 core"}
+                                         f"({sec:.1f} s), interior zone-updates/s on 1 core; value = measured x "
+                                         f"{corr:.3f} (guarded-to-interior zone ratio of the sample over that of "
+                                         f"the workload)"}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -544,7 +588,9 @@ def run_reference_arm(args, wl_name, rank, world):
         res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s, args.warmup) for s in range(cores)])
     wall = time.perf_counter() - t0
     kind = res[0][0]
-    value = float(sum(r[1] for r in res))
+    measured = float(sum(r[1] for r in res))
+    corr = ghost_factor(n, n_wl)
+    value = measured * corr
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": steps, "warmup": args.warmup, "ms_per_step": float(np.mean([r[2] for r in res]) / steps * 1e3),
@@ -553,8 +599,12 @@ def run_reference_arm(args, wl_name, rank, world):
         "config": {"workload": wl_name, "sample": f"{cores} replicas of a {n}^3 box, same scheme",
                    "scheme": scheme_kw, "cfl": CFL},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "measured_value": measured, "ghost_correction": corr,
                          "sample": f"{cores} concurrent replicas x {steps} steps of a {n}^3 turbulence "
-                                   f"box ({scheme_kw}), interior zone-updates/s summed; wall {wall:.1f} s"},
+                                   f"box ({scheme_kw}), interior zone-updates/s summed; wall {wall:.1f} s; "
+                                   f"value = measured x {corr:.3f}, the ratio of guarded to interior zones "
+                                   f"of the sample to that of the {n_wl[0]}^3 workload (the reference "
+                                   f"advances every guard zone)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -571,6 +621,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-fp64-fmad", action="store_true",
+                    help="leave out the comparator run of the FP64 kernels compiled with FMA contraction")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--layout", default="lean", choices=["standard", "lean"],
                     help="device layout of the FP32 runs of the turbulence workloads (lean: 3D, 144 B per "
@@ -611,19 +663,24 @@ def main():
     if os.path.exists(net_path) and not args.no_learned:
         from ctf_b200.train_c2p import load as load_net
         net = load_net(net_path)
-    # (precision, learned): FP64 first -- its primed MaxLambda sets the dt all runs share
-    runs = [("fp64", False)] if not args.skip_fp64 else []
-    runs.append(("fp32", False))
+    # (key, precision, learned, library variant): FP64 first -- its primed MaxLambda sets the
+    # dt all runs share
+    runs = []
+    if not args.skip_fp64:
+        runs.append(("fp64", "fp64", False, ""))
+        if not args.skip_fp64_fmad:
+            runs.append(("fp64_fmad", "fp64", False, "fmad"))
+    runs.append(("fp32", "fp32", False, ""))
     if net is not None:
-        runs.append(("fp32", True))
+        runs.append(("fp32+learned", "fp32", True, ""))
     results, states, solvers = {}, {}, {}
     dt_fixed = None
     head_key = "fp32+learned" if net is not None else "fp32"
-    for prec, learned in runs:
-        key = prec + ("+learned" if learned else "")
+    zones = int(np.prod(n))
+    for key, prec, learned, variant in runs:
         layout = args.layout if prec == "fp32" else "standard"
         s = Solver(Scheme(precision=prec, learned_c2p=learned, layout=layout, **scheme_kw), n,
-                   stream=stream.cuda_stream)
+                   stream=stream.cuda_stream, lib_variant=variant)
         if learned:
             s.set_c2p_network(net)
         s.upload(P0)
@@ -635,19 +692,23 @@ def main():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+        before = s.stats()
         with ClockSampler(local) as clk:
-            ms, prof = time_device(s, args.steps, args.warmup, dt_fixed, torch, stream)
+            ms, prof, st_warm = time_device(s, args.steps, args.warmup, dt_fixed, torch, stream)
         if dist is not None:
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         st = s.stats()
-        zones = int(np.prod(n))
         results[key] = {"ms_total": ms, "ms_per_step": ms / args.steps,
                         "value": zones * args.steps * world / (ms * 1e-3), "prof": prof, "stats": st,
-                        "clocks": clk.summary()}
-        st_out = s.download()
-        states[key] = st_out if key in ("fp64", head_key) else None
+                        "clocks": clk.summary(),
+                        # the timed steps only (the counters are cumulative since set-up)
+                        "advances": st["advances"] - st_warm["advances"],
+                        "failed_advances": st["failed_advances"] - st_warm["failed_advances"],
+                        "errors": st["failed_zones"] - st_warm["failed_zones"]}
+        del before
+        states[key] = s.download()
         s.profile_disable()
         if key == head_key:
             solvers[key] = s
@@ -661,26 +722,41 @@ def main():
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL,
-                   "layout": f"{args.layout} (FP32 runs); standard (FP64 run)",
+                   "layout": f"{args.layout} (FP32 runs); standard (FP64 runs)",
                    "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
                                 + ("; learned c2p guess (bf16 tcgen05 MLP)" if head_key.endswith("learned") else ""),
                    "dt": dt_fixed, "l2": "every state array > 126 MB L2 (no flush needed)",
                    "parallelism": f"{world} independent replica(s)"},
         "gpu_launches": int(sum(v["launches"] for v in results[head_key]["prof"].values())),
         "clocks": head["clocks"],
+        # failed zones summed over the timed steps of the headline run (Mara.advance's count;
+        # a step that fails is not committed)
+        "errors": head["errors"], "failed_steps": head["failed_advances"],
     }
+
     def c2p_it(k):
         st = results[k]["stats"]
         return st["c2p_iters"] / max(st["c2p_calls"], 1)
     out["runs"] = {k: {"value": r["value"], "ms_per_step": r["ms_per_step"],
-                       "c2p_iters_per_call": c2p_it(k),
+                       "c2p_iters_per_call": c2p_it(k), "errors": r["errors"],
+                       "failed_steps": r["failed_advances"],
                        "kernel_ms_per_step": {c: r["prof"][c]["ms"] / args.steps for c in r["prof"]}}
                    for k, r in results.items()}
     if "fp64" in results:
         out["fp64_plain"] = {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
-                             "clocks": results["fp64"]["clocks"]}
+                             "clocks": results["fp64"]["clocks"],
+                             "build": "--fmad=false: every multiply and add rounded as the reference's build does"}
         out["speedup_vs_fp64"] = head["value"] / results["fp64"]["value"]
         out["l1_rel_vs_fp64"] = rel_l1(states[head_key], states["fp64"], len(n))
+        out["linf_rel_vs_fp64"] = rel_linf(states[head_key], states["fp64"], len(n))
+        if "fp32" in states and head_key != "fp32":
+            out["runs"]["fp32"]["l1_rel_vs_fp64"] = rel_l1(states["fp32"], states["fp64"], len(n))
+        if "fp64_fmad" in results:
+            f = results["fp64_fmad"]
+            out["fp64_fmad"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "clocks": f["clocks"],
+                                "build": "the same FP64 kernels compiled with FMA contraction (not the parity path)",
+                                "linf_rel_vs_fp64": rel_linf(states["fp64_fmad"], states["fp64"], len(n))}
+            out["speedup_vs_fp64_fmad"] = head["value"] / f["value"]
 
     # roofline of the dominant kernel (event-timed inside the timed region)
     peaks = {}
@@ -711,31 +787,30 @@ def main():
     alg_bytes_per_launch = per_unit[dom] * d["units"] / max(d["launches"], 1)
     avg_ms = d["ms"] / max(d["launches"], 1)
     achieved = alg_bytes_per_launch / (avg_ms * 1e-3) / 1e9
-    # DRAM bytes per work unit from one ncu capture of the same kernel on the 160^3 box of
-    # this scheme (profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md,
-    # profiles/k_update_turb160_weno5_hlld_rk3_fp32.md), scaled to this launch's units
-    # (profiles/k_lean_sweep_turb160_weno5_hlld_rk3_fp32.md for the lean sweeps: DRAM bytes per
-    # interior zone, the mean of the x, y and z sweeps)
-    measured = {("flux", "hlld", "standard"): 80.0, ("update", "hlld", "standard"): 219.8,
-                ("flux", "hlld", "lean"): 105.1}
-    tpu = measured.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
+    # DRAM bytes per work unit (face for the standard flux kernel, interior zone otherwise)
+    # from one ncu capture of the same kernel on a 160^3 box of the same scheme -- not this
+    # run -- scaled to this launch's units (lean sweeps: the mean of the x, y and z sweeps)
+    measured = {("flux", "weno5", "hlld", "standard"): 80.0, ("update", "weno5", "hlld", "standard"): 219.8,
+                ("flux", "weno5", "hlld", "lean"): 105.1}
+    measured.update(NCU_TRAFFIC_PER_UNIT)
+    tpu = measured.get((dom, scheme_kw["extrap"], scheme_kw["riemann"], args.layout)) \
+        if head_key.startswith("fp32") else None
     traffic = tpu * d["units"] / max(d["launches"], 1) if tpu else None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                        "frac": achieved / hbm, "traffic": traffic,
-                       "traffic_source": "ncu dram__bytes_read+write per unit at 160^3, scaled" if tpu else None,
+                       "traffic_source": ("ncu dram__bytes_read+write per unit of the same kernel on a 160^3 box "
+                                          "of this scheme (a separate capture, not this run), scaled") if tpu else None,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "kernel_share": {k: prof[k]["ms"] / sum(v["ms"] for v in prof.values()) for k in prof},
                        "algorithmic_bytes_per_unit": per_unit[dom]}
     # What bounds the FP32 HLLD sweeps instead of HBM: instruction issue and latency of the
-    # ~10^3-operation face (ncu figures of the same kernels on the 160^3 box of this scheme)
-    limiter = {("flux", "hlld", "lean"): {"issue_active": 0.467, "fma_pipe": 0.281, "xu_pipe": 0.194,
-                                          "dram_throughput": 0.068,
-                                          "source": "profiles/k_lean_sweep_turb160_weno5_hlld_rk3_fp32.md"},
-               ("flux", "hlld", "standard"): {"issue_active": 0.500, "fma_pipe": 0.292, "xu_pipe": 0.210,
-                                              "source": "profiles/k_flux_turb160_weno5_hlld_rk3_fp32.md"}}
-    lim = limiter.get((dom, scheme_kw["riemann"], args.layout)) if head_key.startswith("fp32") else None
+    # ~10^3-operation face (ncu figures of the same kernel on a 160^3 box of the same scheme,
+    # from a separate capture, not this run)
+    lim = NCU_LIMITER.get((dom, scheme_kw["extrap"], scheme_kw["riemann"], args.layout)) \
+        if head_key.startswith("fp32") else None
     if lim:
-        out["roofline"]["limiter"] = {"kind": "instruction issue / latency (FP32 pipes)", **lim}
+        out["roofline"]["limiter"] = {"kind": "instruction issue / latency (FP32 pipes)", **lim,
+                                      "source": "ncu capture of the same kernel on a 160^3 box, not this run"}
     # The whole step against HBM: the compulsory state-vector transfers of one zone-update
     # (single 2, RK2 5, RK3 8: each stage reads its register(s) and writes one) times the bytes
     # of a state vector (64 B FP64; 44 B FP32 bulk with the FP64 field), at the headline rate
@@ -767,10 +842,12 @@ def main():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+        e2e_err = 0
         t0 = time.perf_counter()
         for _ in range(args.steps):
             dt = solver_fp32.get_timestep(CFL)
             _, e = solver_fp32.advance_host(host, min(dt, dt_fixed))
+            e2e_err += e
         sec = time.perf_counter() - t0
         if dist is not None:
             t = torch.tensor([sec], device="cuda")
@@ -778,15 +855,20 @@ def main():
             sec = float(t.item())
         nbytes = int(np.prod(solver_fp32.shape)) * 8
         out["e2e"] = {"value": int(np.prod(n)) * args.steps * world / sec, "unit": UNIT,
-                      "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                      "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "errors": e2e_err,
                       "api": "mgpu_advance_host (Mara.advance(buf, dt)) + mgpu_get_timestep"}
     solver_fp32.close()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        kind, v, sec = cpu_sample(scheme_kw, steps=2, n=48)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
-                               "sample": f"48^3 turbulence box, same scheme, 2 steps after priming "
-                                         f"({sec:.1f} s), interior zone-updates/s on 1 core"}
+        ns_cpu = 48
+        kind, v, sec = cpu_sample(scheme_kw, steps=2, n=ns_cpu)
+        corr = ghost_factor(ns_cpu, n)
+        out["cpu_baseline"] = {"value": v * corr, "unit": UNIT, "cores": 1, "kind": kind,
+                               "measured_value": v, "ghost_correction": corr,
+                               "sample": f"{ns_cpu}^3 turbulence box, same scheme, 2 steps after priming "
+                                         f"({sec:.1f} s), interior zone-updates/s on 1 core; value = measured x "
+                                         f"{corr:.3f}, the ratio of guarded to interior zones of the sample to that "
+                                         f"of the {n[0]}^3 workload (the reference advances every guard zone)"}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

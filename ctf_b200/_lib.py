@@ -14,8 +14,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libmaragpu.so")
 CSRC = os.path.join(HERE, "csrc")
 
+# The FP64 kernels built with FMA contraction on (a comparator, not the parity path).
+LIB_FMAD_PATH = os.path.join(HERE, "_lib", "libmaragpu_fmad.so")
+
 _lock = threading.Lock()
 _lib = None
+_lib_fmad = None
 
 
 class MgpuConfig(ctypes.Structure):
@@ -33,7 +37,8 @@ class MgpuStats(ctypes.Structure):
                 ("c2p_iters", ctypes.c_ulonglong), ("c2p_attempt", ctypes.c_ulonglong * 6),
                 ("face_c2p_calls", ctypes.c_ulonglong), ("face_c2p_iters", ctypes.c_ulonglong),
                 ("hlld_ok", ctypes.c_ulonglong), ("hlld_hllc", ctypes.c_ulonglong),
-                ("pcm_retry", ctypes.c_ulonglong)]
+                ("pcm_retry", ctypes.c_ulonglong), ("advances", ctypes.c_ulonglong),
+                ("failed_advances", ctypes.c_ulonglong), ("failed_zones", ctypes.c_ulonglong)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "c2p_attempt"}
@@ -144,17 +149,34 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def load() -> ctypes.CDLL:
-    """Load the library (building it first if it is absent); raises if that fails."""
-    global _lib
+def _bind(path: str) -> ctypes.CDLL:
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def load(variant: str = "") -> ctypes.CDLL:
+    """Load the library (building it first if it is absent); raises if that fails.
+
+    variant "fmad" loads libmaragpu_fmad.so, whose FP64 kernels are compiled with FMA
+    contraction on: the comparator of an FP64 build that uses fused multiply-adds.  It is not
+    the parity path (the plain FP64 path rounds every multiply and add as the reference
+    does)."""
+    global _lib, _lib_fmad
     with _lock:
+        if variant == "fmad":
+            if _lib_fmad is None:
+                if not os.path.exists(LIB_FMAD_PATH):
+                    build(force=True)
+                _lib_fmad = _bind(LIB_FMAD_PATH)
+            return _lib_fmad
+        if variant:
+            raise ValueError(f"no library variant {variant!r}")
         if _lib is None:
             if not os.path.exists(LIB_PATH):
                 build()
-            lib = ctypes.CDLL(LIB_PATH)
-            for name, (res, args) in SIGNATURES.items():
-                fn = getattr(lib, name)
-                fn.restype = res
-                fn.argtypes = args
-            _lib = lib
+            _lib = _bind(LIB_PATH)
         return _lib

@@ -16,7 +16,6 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
-#include <mutex>
 
 #include "../../include/mara_gpu.h"
 #include "rmhd_types.cuh"
@@ -43,10 +42,6 @@ static_assert(CS_MAX % 32 == 0, "component stride must be a multiple of 32");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 namespace {
-
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_lock;
-void *g_scratch_addr[MAX_DEVICES] = {nullptr};
 
 void put_err(char *buf, int len, const char *msg)
 {
@@ -112,29 +107,23 @@ extern "C" int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, co
   g.dz = (hi[2] - lo[2]) / (g.G[2] - 2 * ng);
   g.ninterior = (long long) g.n[0] * g.n[1] * g.n[2];
 
-  // Set-up, once per device, with that device current: the device address of the scratch
-  // array (the host-side name g_noalloc_scratch is not a device address).
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
-    put_err(errbuf, errbuf_len, "mgpu_advance_noalloc: no usable CUDA device");
-    return MGPU_ERR_CUDA;
-  }
+  // Set-up, on every call, with the caller's device current: the device address of the
+  // scratch array (the host-side name g_noalloc_scratch is not a device address).  It is
+  // looked up each time rather than cached, because a cudaDeviceReset or another context on
+  // the same device between two calls would leave a cached address stale.  The lookup is a
+  // table read once the library's device code is loaded; the first call on a device loads it.
   unsigned char *base;
   {
-    std::lock_guard<std::mutex> lock(g_setup_lock);
-    if (!g_scratch_addr[dev]) {
-      void *p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        char msg[200];
-        snprintf(msg, sizeof(msg), "mgpu_advance_noalloc: cudaGetSymbolAddress failed: %s",
-                 cudaGetErrorString(e));
-        put_err(errbuf, errbuf_len, msg);
-        return MGPU_ERR_CUDA;
-      }
-      g_scratch_addr[dev] = p;
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      char msg[200];
+      snprintf(msg, sizeof(msg), "mgpu_advance_noalloc: cudaGetSymbolAddress failed: %s",
+               cudaGetErrorString(e));
+      put_err(errbuf, errbuf_len, msg);
+      return MGPU_ERR_CUDA;
     }
-    base = (unsigned char *) g_scratch_addr[dev];
+    base = (unsigned char *) p;
   }
 
   // Carve the scratch into the advance's arrays (sized for the largest box, CS_MAX).

@@ -114,12 +114,20 @@ static __global__ void k_begin(Ctl *ctl, int dt_mode, double dt, double cfl, dou
 static __global__ void k_commit(Ctl *ctl, int nstages)
 {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    int e = 0;
-    for (int s = 0; s < nstages; ++s) e |= ctl->stage_err[s];
+    int e = 0, first = 0;
+    for (int s = 0; s < nstages; ++s) {
+      e |= ctl->stage_err[s];
+      if (!first) first = ctl->stage_err[s];
+    }
     e |= ctl->final_err;
+    if (!first) first = ctl->final_err;
+    ctl->n_advances += 1;
     if (e == 0) {
       ctl->cur ^= 1;
       ctl->committed = 1;
+    } else {
+      ctl->n_failed += 1;
+      ctl->n_failed_zones += (unsigned) first;
     }
   }
 }

@@ -72,6 +72,9 @@ struct Ctl {
   int ctu_err[4];
   int ctu_c2p_err;
   int ctu_reset;
+  // since the solver was created (never reset by an advance): advances run, advances not
+  // committed, and the failed zones those reported (as Mara.advance returns them)
+  unsigned long long n_advances, n_failed, n_failed_zones;
   // statistics, accumulated over the advance
   StatSlot stat[STAT_SLOTS];
 };

@@ -88,8 +88,8 @@ class Scheme:
 class Solver:
     """One GPU solver handle with a device-resident primitive state."""
 
-    def __init__(self, scheme: Scheme, n, x0=None, x1=None, ng: int = 3, stream=None):
-        self.lib = _lib.load()
+    def __init__(self, scheme: Scheme, n, x0=None, x1=None, ng: int = 3, stream=None, lib_variant: str = ""):
+        self.lib = _lib.load(lib_variant)
         self.scheme = scheme
         h = ctypes.c_void_p()
         cfg = scheme.to_config()

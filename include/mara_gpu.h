@@ -83,6 +83,9 @@ typedef struct {
   unsigned long long face_c2p_calls, face_c2p_iters; /* HLL-state c2p inside HLLD */
   unsigned long long hlld_ok, hlld_hllc, pcm_retry;  /* HLLD successes / HLLC fallbacks /
                                                         PCM retries of a face */
+  unsigned long long advances, failed_advances,      /* since mgpu_set_domain: advances run, those */
+                     failed_zones;                   /* not committed, and the failed zones
+                                                        they reported (sum of their `errors`) */
 } mgpu_stats;
 
 /* Defaults of a freshly started reference plus set_fluid('rmhd'), gamma 4/3, PLM theta 2,
@@ -236,10 +239,12 @@ int mgpu_halo_unpack(mgpu_solver *h, int which, int dim, int side, const void *d
  * life of the process) instead of cudaMalloc.  The caller passes device AoS primitives with
  * guard zones in (dev_prim_in) and out (dev_prim_out, written only when *errors == 0) and a
  * stream (NULL = the default stream); cfg must select MGPU_PREC_FP64 without learned_c2p;
- * Ng is 3.  The call is synchronous and returns the reference's error count and MaxLambda.
- * Larger boxes are rejected with MGPU_ERR_ARG and a message in errbuf.  The first call on
- * each device looks up that device's address of the region (cudaGetSymbolAddress); make it
- * before any stream capture.  All calls share the region: calls whose work overlaps on the
+ * Ng is 3.  The call is synchronous (it returns after its work on the stream has finished)
+ * and returns the reference's error count and MaxLambda.  Larger boxes are rejected with
+ * MGPU_ERR_ARG and a message in errbuf.  Every call looks up the current device's address of
+ * the region (cudaGetSymbolAddress, with that device current), so a cudaDeviceReset or
+ * another context between calls is harmless; the first call on a device also loads the
+ * library's device code there.  All calls share the region: calls whose work overlaps on the
  * GPU (several streams or host threads) race and must be serialised by the caller. */
 #define MGPU_NOALLOC_MAX_ZONES 11520
 int mgpu_advance_noalloc(const mgpu_config *cfg, const double *x0, const double *x1, const int *N, int nd,

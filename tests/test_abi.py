@@ -119,3 +119,69 @@ def test_ensemble_box_sizes_are_log_uniform():
     # log-uniform: the median side is near the geometric mean sqrt(64 * 512) = 181
     assert 150 <= np.median(sides) <= 215
     assert kh_sizes(256, seed=0) == sizes
+
+
+def _noalloc_call(lib, cfg, n, errbuf, nd=None, src=16, dst=16, x0=True):
+    """mgpu_advance_noalloc with placeholder device pointers: every argument check returns
+    before the call touches the device, so this runs without a GPU."""
+    nd = len(n) if nd is None else nd
+    m = max(nd, 1)
+    X0 = (ctypes.c_double * m)(*([0.0] * m)) if x0 else None
+    X1 = (ctypes.c_double * m)(*([1.0] * m))
+    N = (ctypes.c_int * m)(*(list(n) + [8] * m)[:m])
+    err, ml = ctypes.c_int(-1), ctypes.c_double(0.0)
+    return lib.mgpu_advance_noalloc(ctypes.byref(cfg), X0, X1, N, nd, ctypes.c_void_p(src),
+                                    ctypes.c_void_p(dst), ctypes.c_double(1e-3), ctypes.byref(err),
+                                    ctypes.byref(ml), None, errbuf, len(errbuf))
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("precision", 1, "needs an rmhd FP64 plm-split configuration"),
+    ("learned_c2p", 1, "needs an rmhd FP64 plm-split configuration"),
+    ("godunov", 1, "needs an rmhd FP64 plm-split configuration"),
+    ("layout", 1, "needs an rmhd FP64 plm-split configuration"),
+    ("rk", 5, "needs an rmhd FP64 plm-split configuration"),
+    ("gamma", 1.0, "needs an rmhd FP64 plm-split configuration"),
+])
+def test_noalloc_config_checks_without_a_gpu(field, value, msg):
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    setattr(c, field, value)
+    buf = ctypes.create_string_buffer(256)
+    assert _noalloc_call(lib, c, (8, 8, 8), buf) == 1      # MGPU_ERR_ARG
+    assert msg in buf.value.decode()
+
+
+@pytest.mark.parametrize("case,msg", [
+    ("nd0", "1, 2 or 3 dimensions"),
+    ("nd4", "1, 2 or 3 dimensions"),
+    ("small_axis", "needs N >= 3 on every axis"),
+    ("too_many_zones", "more than the 11520"),
+    ("null_input", "null argument"),
+    ("null_output", "null argument"),
+    ("null_extent", "null argument"),
+])
+def test_noalloc_domain_checks_without_a_gpu(case, msg):
+    lib = _lib.load()
+    c = _lib.MgpuConfig()
+    lib.mgpu_default_config(ctypes.byref(c))
+    buf = ctypes.create_string_buffer(256)
+    kw = {}
+    n = (8, 8, 8)
+    if case == "nd0":
+        kw["nd"] = 0
+    elif case == "nd4":
+        n, kw["nd"] = (8, 8, 8, 8), 4
+    elif case == "small_axis":
+        n = (8, 2, 8)
+    elif case == "too_many_zones":
+        n = (20, 20, 20)
+    elif case == "null_input":
+        kw["src"] = None
+    elif case == "null_output":
+        kw["dst"] = None
+    else:
+        kw["x0"] = False
+    assert _noalloc_call(lib, c, n, buf, **kw) == 1
+    assert msg in buf.value.decode()

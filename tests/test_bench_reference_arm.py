@@ -37,3 +37,25 @@ def test_reference_arm_json_contract(workload):
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+
+
+def test_default_workload_is_the_512_plm_hlld_rk3_box():
+    import bench
+    n, ic, kw = bench.WORKLOADS[bench.DEFAULT_WORKLOAD]
+    assert n == (512, 512, 512) and ic == "turbulence"
+    assert kw == dict(extrap="plm", riemann="hlld", advance="rk3")
+
+
+def test_ghost_correction_and_linf():
+    import numpy as np
+    import bench
+    assert bench.ghost_factor(64, (64, 64, 64)) == 1.0
+    # 64^3 sample (70^3 guarded) against a 512^3 box (518^3 guarded)
+    want = (70 / 64) ** 3 / (518 / 512) ** 3
+    assert abs(bench.ghost_factor(64, (512, 512, 512)) - want) < 1e-12
+    a = np.ones((10, 10, 10, 8))
+    b = a.copy()
+    b[5, 5, 5, 0] = 1.5            # interior zone
+    b[0, 0, 0, 1] = 9.0            # guard zone: not counted
+    r = bench.rel_linf(a, b, 3)
+    assert abs(r["rho"] - 0.5 / 1.5) < 1e-15 and r["pre"] == 0.0

@@ -48,6 +48,8 @@ def _noalloc(lib, cfg, n, src, dst, dt):
 @pytest.mark.parametrize("scheme_kw,n", [
     (dict(extrap="plm", riemann="hlld", advance="rk2"), (10, 12, 14)),
     (dict(extrap="weno5", riemann="hllc", advance="rk3"), (40, 36)),
+    (dict(extrap="plm", riemann="hll", advance="rk4"), (9, 8, 11)),     # the K registers
+    (dict(extrap="weno5", riemann="hlld", advance="single"), (200,)),   # a 1D box
 ])
 def test_noalloc_matches_regular_entry_point_twice(scheme_kw, n):
     import torch
@@ -55,7 +57,13 @@ def test_noalloc_matches_regular_entry_point_twice(scheme_kw, n):
     lib = _lib.load()
     scheme = Scheme(**scheme_kw)
     cfg = scheme.to_config()
-    P0 = ics.turbulence_box(n, seed=21) if len(n) == 3 else ics.kh_box(n, seed=21)
+    if len(n) == 3:
+        P0 = ics.turbulence_box(n, seed=21)
+    elif len(n) == 2:
+        P0 = ics.kh_box(n, seed=21)
+    else:   # a line across the layers of a 2D shear box, laid along x: a 1D state whose
+        # density, velocity and field all vary
+        P0 = np.ascontiguousarray(ics.kh_box((8, n[0]), seed=21)[5].reshape(n[0] + 6, 1, 1, 8))
 
     ref = Solver(scheme, n)
     ref.upload(P0.copy())
@@ -67,6 +75,7 @@ def test_noalloc_matches_regular_entry_point_twice(scheme_kw, n):
     d_mid = torch.zeros_like(d_in)
     d_out = torch.zeros_like(d_in)
     torch.cuda.synchronize()
+    free_before = None
     for src, dst in ((d_in, d_mid), (d_mid, d_out)):
         assert ref.advance(dt) == 0
         rc, errors, ml, msg = _noalloc(lib, cfg, n, src.data_ptr(), dst.data_ptr(), dt)
@@ -76,6 +85,12 @@ def test_noalloc_matches_regular_entry_point_twice(scheme_kw, n):
         assert abs(ml - ref.max_lambda) <= 1e-12 * ref.max_lambda
         got = dst.cpu().numpy()
         assert _rel_linf(got, ref.download()) <= STEP_TOL
+        # the property that defines this entry point: after the first call (which may load
+        # the library's device code), a call takes no device memory
+        free = torch.cuda.mem_get_info()[0]
+        if free_before is not None:
+            assert free == free_before, (free_before, free)
+        free_before = free
 
 
 def test_noalloc_rejects_boxes_beyond_its_limit():

@@ -139,6 +139,26 @@ SIGNATURES = {
                                                   ctypes.POINTER(ctypes.c_longlong)]),
     "mgpu_ensemble_time_advance": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuEnsembleLaunch), _dp, ctypes.c_int, _dp]),
     "mgpu_ensemble_autotune": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.POINTER(MgpuEnsembleLaunch), _dp]),
+    "mgpu_probe_prim_to_cons": (ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_longlong, _vp, _vp]),
+    "mgpu_probe_c2p": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _vp, _vp, ctypes.c_longlong,
+                                      _vp, _vp, _vp]),
+    "mgpu_probe_flux": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, _vp, ctypes.c_longlong, _vp, _vp]),
+    "mgpu_probe_riemann": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double, _vp,
+                                          _vp, ctypes.c_longlong, _vp, _vp, _vp, _vp]),
+    "mgpu_probe_reconstruct": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, _vp,
+                                              ctypes.c_longlong, _vp]),
+    "mgpu_measure_mean_cons": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_mean_prim": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_mean_energies": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_mean_velocity": (ctypes.c_int, [_vp, _dp]),
+    "mgpu_measure_mean_max_temperature": (ctypes.c_int, [_vp, _dp, _dp]),
+    "mgpu_measure_mean_max_magnetic_field": (ctypes.c_int, [_vp, _dp, _dp]),
+    "mgpu_measure_mean_max_sonic_mach": (ctypes.c_int, [_vp, _dp, _dp]),
+    "mgpu_measure_mean_min_alfvenic_mach": (ctypes.c_int, [_vp, _dp, _dp]),
+    "mgpu_diffuse": (ctypes.c_int, [_vp, ctypes.c_double, _ip]),
+    "mgpu_diffuse_host": (ctypes.c_int, [_vp, _dp, ctypes.c_double, _ip]),
+    "mgpu_set_failmask": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "mgpu_reconfigure": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuConfig)]),
 }
 
 

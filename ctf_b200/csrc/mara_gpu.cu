@@ -2,6 +2,7 @@
 // C ABI declared in include/mara_gpu.h.  Kernels live in kernels_fp64.cu (compiled with
 // --fmad=false) and kernels_fp32.cu.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -18,6 +19,7 @@ MGPU_DECLARE_PRECISION(fp32)
 using namespace mgpu;
 
 #include "solver.h"
+#include "measures.h"
 
 namespace {
 
@@ -67,6 +69,8 @@ void free_buffers(mgpu_solver *h)
   h->b = AdvanceBuffers{};
   h->staging = nullptr;
   h->red = nullptr;
+  h->meas = nullptr;
+  h->fmask = nullptr;
 }
 
 cudaError_t dalloc(mgpu_solver *h, void **p, size_t bytes)
@@ -263,11 +267,13 @@ int mgpu_create(const mgpu_config *cfg, mgpu_solver **out)
   if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(Ctl));
   if (e == cudaSuccess) e = cudaMallocHost((void **) &h->ctl_host, sizeof(Ctl));
   if (e == cudaSuccess) e = cudaMallocHost((void **) &h->red_host, sizeof(double) * 2 * RED_BLOCKS);
+  if (e == cudaSuccess) e = cudaMallocHost((void **) &h->meas_host, sizeof(double) * MEAS_BLOCKS * MEAS_FIELDS);
   if (e != cudaSuccess) {
     fprintf(stderr, "[mgpu] CUDA unavailable: %s\n", cudaGetErrorString(e));
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->ctl) cudaFree(h->ctl);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
+    if (h->red_host) cudaFreeHost(h->red_host);
     delete h;
     return MGPU_ERR_CUDA;
   }
@@ -289,6 +295,7 @@ int mgpu_destroy(mgpu_solver *h)
   if (h->ctl) cudaFree(h->ctl);
   if (h->ctl_host) cudaFreeHost(h->ctl_host);
   if (h->red_host) cudaFreeHost(h->red_host);
+  if (h->meas_host) cudaFreeHost(h->meas_host);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return MGPU_OK;
@@ -384,7 +391,14 @@ int mgpu_set_domain(mgpu_solver *h, const double *x0, const double *x1, const in
   h->staging_zones = g.nz < (1ll << 22) ? g.nz : (1ll << 22);   // up to 256 MB of AoS
   if (e == cudaSuccess) e = dalloc(h, (void **) &h->staging, (size_t) h->staging_zones * 8 * sizeof(double));
   if (e == cudaSuccess) e = dalloc(h, (void **) &h->red, sizeof(double) * 2 * RED_BLOCKS);
+  if (e == cudaSuccess) e = dalloc(h, (void **) &h->meas, sizeof(double) * MEAS_BLOCKS * MEAS_FIELDS);
+  // the failure mask of the last c2p (one byte per guarded zone; not kept in the lean layout,
+  // whose Mara.diffuse is not offered)
+  h->fmask = nullptr;
+  if (e == cudaSuccess && !lean(h)) e = dalloc(h, (void **) &h->fmask, (size_t) g.nz);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->ctl, 0, sizeof(Ctl), h->stream);
+  if (e == cudaSuccess && h->fmask)
+    e = cudaMemcpyAsync(&h->ctl->fmask, &h->fmask, sizeof(h->fmask), cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     free_buffers(h);
@@ -490,7 +504,7 @@ int mgpu_set_primitive(mgpu_solver *h, const double *host_aos)
   return transfer(h, const_cast<double *>(host_aos), nullptr, nullptr, 2);
 }
 
-static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
+static AdvanceArgs advance_args(mgpu_solver *h, int dt_mode, double dt, double cfl)
 {
   AdvanceArgs A;
   A.g = h->g;
@@ -509,6 +523,12 @@ static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
   A.ctl = h->ctl;
   A.stream = h->stream;
   A.prof = h->prof_on ? &h->prof : nullptr;
+  return A;
+}
+
+static int enqueue_advance(mgpu_solver *h, int dt_mode, double dt, double cfl)
+{
+  const AdvanceArgs A = advance_args(h, dt_mode, dt, cfl);
   cudaError_t e = fp32(h) ? advance_fp32(A) : advance_fp64(A);
   CK(e);
   CK(mgpu_driving_enqueue(h));
@@ -687,6 +707,223 @@ int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax)
   double mx = 0.0;
   for (int b = 0; b < RED_BLOCKS; ++b) mx = fmax(mx, h->red_host[b]);
   *wmax = mx;
+  return MGPU_OK;
+}
+
+// ---- the other Mara.measure.* (Mara/mara.cpp:1954-2230): one device pass, host sums ----------
+namespace {
+
+// PhysicalUnits(1, 1, 1) (cgs), the units a started reference holds (Mara/hydro.cpp:20), as
+// Mara/units.cpp computes them.
+MeasureUnits default_units()
+{
+  const double length = 1.0, mass = 1.0, time = 1.0;
+  const double gram = 1.0 / mass, centimeter = 1.0 / length, second = 1.0 / time;
+  const double erg = gram * pow(centimeter / second, 2.0);
+  const double mev = 1.60217648740e-06 * erg;                       // MEV_TO_ERG (Mara/eos.hpp:15)
+  const double mev_fm3 = mev / pow(1e-13 * centimeter, 3);
+  MeasureUnits u;
+  u.erg_cc = mev_fm3 * 1e-33;
+  u.gcc = gram / pow(centimeter, 3.0);
+  const double mp = 1.67262177774e-24 * gram;                        // PROTON_MASS
+  const double kb = 1.38064881300e-16 * erg;                         // BOLTZMANN_CONSTANT
+  u.mp_kb = mp / kb;
+  u.gauss = sqrt(erg / pow(centimeter, 3.0) / (4 * M_PI));
+  return u;
+}
+
+// Runs the reduction over the measured primitive array and sums the block partials in block
+// order: out[MEAS_FIELDS] (sums, then the extremes).  ttl = the global interior zone count.
+int measure_all(mgpu_solver *h, double *out, double *ttl, MeasureUnits *units)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  const MeasureUnits u = default_units();
+  CK(measures_launch(h->g, h->b.PA, fp32(h), h->cfg.gamma, u, h->meas, h->stream));
+  CK(cudaMemcpyAsync(h->meas_host, h->meas, sizeof(double) * MEAS_BLOCKS * MEAS_FIELDS, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int q = 0; q < MEAS_FIELDS; ++q) {
+    double v = q < MEAS_SUMS ? 0.0 : h->meas_host[q];
+    for (int b = q < MEAS_SUMS ? 0 : 1; b < MEAS_BLOCKS; ++b) {
+      const double x = h->meas_host[(size_t) b * MEAS_FIELDS + q];
+      if (q < MEAS_SUMS) v += x;
+      else if (q == MEAS_MAMIN) v = x < v ? x : v;
+      else v = x > v ? x : v;
+    }
+    out[q] = v;
+  }
+  long long glb = 1;
+  for (int d = 0; d < h->g.nd; ++d) glb *= h->N[d];
+  *ttl = (double) glb;
+  if (units) *units = u;
+  return MGPU_OK;
+}
+
+}  // namespace
+
+int mgpu_measure_mean_cons(mgpu_solver *h, double *out)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!out) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  for (int q = 0; q < 8; ++q) out[q] = m[MEAS_CONS + q] / ttl;
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_prim(mgpu_solver *h, double *out)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!out) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  for (int q = 0; q < 8; ++q) out[q] = m[MEAS_PRIM + q] / ttl;
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_energies(mgpu_solver *h, double *out)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!out) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  for (int q = 0; q < 4; ++q) out[q] = m[MEAS_ENERGY + q] / ttl;
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_velocity(mgpu_solver *h, double *out)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!out) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  for (int q = 0; q < 4; ++q) out[q] = m[MEAS_VEL + q] / ttl;
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_max_temperature(mgpu_solver *h, double *mean, double *max)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!mean || !max) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  *mean = m[MEAS_T] / ttl;
+  *max = m[MEAS_TMAX];
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_max_magnetic_field(mgpu_solver *h, double *mean, double *max)
+{
+  double m[MEAS_FIELDS], ttl;
+  MeasureUnits u;
+  if (!mean || !max) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, &u);
+  if (rc) return rc;
+  *mean = (1.0 / u.gauss) * m[MEAS_B] / ttl;
+  *max = (1.0 / u.gauss) * m[MEAS_BMAX];
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_max_sonic_mach(mgpu_solver *h, double *mean, double *max)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!mean || !max) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  *mean = m[MEAS_MS] / ttl;
+  *max = m[MEAS_MSMAX];
+  return MGPU_OK;
+}
+
+int mgpu_measure_mean_min_alfvenic_mach(mgpu_solver *h, double *mean, double *min)
+{
+  double m[MEAS_FIELDS], ttl;
+  if (!mean || !min) return MGPU_ERR_ARG;
+  const int rc = measure_all(h, m, &ttl, nullptr);
+  if (rc) return rc;
+  *mean = m[MEAS_MA] / ttl;
+  *min = m[MEAS_MAMIN];
+  return MGPU_OK;
+}
+
+// ---- Mara.diffuse / Mara.set_failmask (Mara/mara.cpp:343-373) ----------------------------------
+static int diffuse_ready(mgpu_solver *h)
+{
+  int rc = ensure_ready(h);
+  if (rc) return rc;
+  if (lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "diffuse is not offered in the lean layout");
+  for (int d = 0; d < 3; ++d)
+    if (h->g.ext[d]) return fail(h, MGPU_ERR_UNSUPPORTED, "diffuse needs a single (undecomposed) domain");
+  return MGPU_OK;
+}
+
+int mgpu_diffuse(mgpu_solver *h, double r, int *errors)
+{
+  int rc = diffuse_ready(h);
+  if (rc) return rc;
+  const AdvanceArgs A = advance_args(h, 0, 0.0, 0.0);
+  CK(fp32(h) ? diffuse_fp32(A, r) : diffuse_fp64(A, r));
+  rc = read_ctl(h);
+  if (rc) return rc;
+  if (errors) *errors = h->ctl_host->diffuse_err;
+  return MGPU_OK;
+}
+
+int mgpu_diffuse_host(mgpu_solver *h, double *host_aos, double r, int *errors)
+{
+  int rc = diffuse_ready(h);
+  if (rc) return rc;
+  rc = mgpu_upload_prim(h, host_aos);
+  if (rc) return rc;
+  rc = mgpu_diffuse(h, r, errors);
+  if (rc) return rc;
+  return mgpu_download_prim(h, host_aos);
+}
+
+int mgpu_set_failmask(mgpu_solver *h, int value)
+{
+  int rc = diffuse_ready(h);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(h->fmask, value != 0, (size_t) h->g.nz, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MGPU_OK;
+}
+
+int mgpu_reconfigure(mgpu_solver *h, const mgpu_config *cfg)
+{
+  if (!h || !cfg) return MGPU_ERR_ARG;
+  mgpu_solver probe;
+  int rc = check_config(&probe, cfg);
+  if (rc) return fail(h, rc, probe.err);
+  const mgpu_config &c = h->cfg;
+  if (cfg->fluid != c.fluid || cfg->precision != c.precision || cfg->layout != c.layout)
+    return fail(h, MGPU_ERR_UNSUPPORTED, "reconfigure keeps the fluid, precision and layout of the solver");
+  if (h->have_domain) {
+    for (int d = 0; d < 3; ++d)
+      if (h->g.ext[d] && cfg->godunov == MGPU_GODUNOV_PLM_MUSCL)
+        return fail(h, MGPU_ERR_UNSUPPORTED, "'plm-muscl' needs a single domain");
+    CK(cudaStreamSynchronize(h->stream));
+    const size_t cs = (size_t) h->g.cs, tsz = fp32(h) ? sizeof(float) : sizeof(double);
+    cudaError_t e = cudaSuccess;
+    if (cfg->rk == 4 && !h->b.K_bulk[0])
+      for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+        e = dalloc(h, &h->b.K_bulk[i], 5 * cs * tsz);
+        if (e == cudaSuccess) e = dalloc(h, (void **) &h->b.K_B[i], 3 * cs * sizeof(double));
+      }
+    if (cfg->godunov == MGPU_GODUNOV_PLM_MUSCL && !h->b.Pd[0])
+      for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+        if (d < h->g.nd) e = dalloc(h, &h->b.Pd[d], 8 * cs * tsz);
+        else h->b.Pd[d] = h->b.Pd[0];
+      }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, e == cudaErrorMemoryAllocation ? MGPU_ERR_NOMEM : MGPU_ERR_CUDA,
+                  std::string("reconfigure: ") + cudaGetErrorString(e));
+    }
+  }
+  h->cfg = *cfg;
   return MGPU_OK;
 }
 

@@ -9,6 +9,7 @@
 #include "rmhd_step_tc.cuh"
 #include "rmhd_ctu.cuh"
 #include "rmhd_lean.cuh"
+#include "rmhd_diffuse.cuh"
 
 #ifndef MGPU_TC_CTAS_PER_SM
 #define MGPU_TC_CTAS_PER_SM 4
@@ -391,4 +392,5 @@ inline cudaError_t launch_halo(const TransferArgs &A, int which, int dim, int si
   { return launch_face_io<T>(A, d_aos, z0, count, to_aos); }                                             \
   cudaError_t halo_##suffix(const TransferArgs &A, int which, int dim, int side, void *buf, int pack)     \
   { return launch_halo<T>(A, which, dim, side, buf, pack); }                                             \
+  cudaError_t diffuse_##suffix(const AdvanceArgs &A, double r) { return launch_diffuse<T>(A, r); }       \
   }

@@ -172,7 +172,7 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
                                            const double *u, double *p, int err, const C2PTally &tally)
 {
   const bool counted = final != C2P_LEAN_RESTORE;
-  if (counted) {
+  if (counted && final != C2P_DIFFUSE) {
     StatSlot &st = stat_slot(ctl);
     warp_add(&st.c2p_calls, 1u);
     warp_add(&st.c2p_iters, (unsigned) tally.iters);
@@ -187,12 +187,17 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
       p[6] = u[6];
       p[7] = u[7];
       if (final == 2) atomicAdd(&ctl->ctu_reset, 1);
+    } else if (final == C2P_DIFFUSE) {
+      atomicAdd(&ctl->diffuse_err, multiplicity(g, i, j, k));
     } else if (counted) {
       const bool closing = final == C2P_CLOSING || final == C2P_LEAN_CLOSING;
       atomicAdd(closing ? &ctl->final_err : final == C2P_CTU_STAGE ? &ctl->ctu_c2p_err : &ctl->stage_err[stage],
                 multiplicity(g, i, j, k));
     }
   }
+  // the failure mask of this c2p at the zone and its images (an emergency reset clears it)
+  unsigned char *const fm = counted ? ctl->fmask : nullptr;
+  const unsigned char failed = (unsigned char) (err && !ereset);
   int pi[3], pj[3], pk[3];
   const int ni = images_1d(i, g.n[0], g.ng, self_periodic(g, 0), pi);
   const int nj = images_1d(j, g.n[1], g.ng, self_periodic(g, 1), pj);
@@ -201,7 +206,8 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
     for (int b = 0; b < nj; ++b)
       for (int c = 0; c < nk; ++c) {
         const long long w = ((long long) pi[a] * g.G[1] + pj[b]) * g.G[2] + pk[c];
-        if (final == 1) {
+        if (fm) fm[w] = failed;
+        if (final == C2P_CLOSING || final == C2P_DIFFUSE) {
 #pragma unroll
           for (int q = 0; q < 5; ++q) Pn.bulk[q * g.cs + w] = T(p[q]);
 #pragma unroll
@@ -224,7 +230,7 @@ template <class T>
 __device__ __forceinline__ StateCPtr<T> c2p_input(const Ctl *ctl, int final, StateCPtr<T> U, StatePtr<T> Pn0,
                                                   StatePtr<T> Pn1)
 {
-  if (final < C2P_LEAN_STAGE) return U;
+  if (final < C2P_LEAN_STAGE || final == C2P_DIFFUSE) return U;
   const int r = final == C2P_LEAN_RESTORE ? ctl->cur : ctl->cur ^ 1;
   const StatePtr<T> R = r ? Pn1 : Pn0;
   return StateCPtr<T>{R.bulk, R.B};
@@ -268,7 +274,9 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, Sta
   if (c2p_skip(ctl, stage, final)) return;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.ninterior) return;
-  c2p_zone<T, Guess>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, ctl->cur ? Pn0 : Pn1, pp, ctl, stage, zero_guess,
+  // the uncommitted buffer, or for Mara.diffuse the committed one (rewritten in place)
+  const int target = final == C2P_DIFFUSE ? ctl->cur : ctl->cur ^ 1;
+  c2p_zone<T, Guess>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess,
                      final, ereset, preset, dreset, t);
 }
 

@@ -54,7 +54,9 @@ enum C2PMode {
   // lean layout: the conserved registers are U[cur] (committed) and U[!cur] (RK register)
   C2P_LEAN_STAGE = 3,     // U[!cur] -> PA
   C2P_LEAN_CLOSING = 4,   // U[!cur] -> PA, plus its field to U[!cur]'s guard images
-  C2P_LEAN_RESTORE = 5    // U[cur] -> PA after an advance that did not commit; uncounted
+  C2P_LEAN_RESTORE = 5,   // U[cur] -> PA after an advance that did not commit; uncounted
+  C2P_DIFFUSE = 6         // Mara.diffuse: U -> the committed buffer in place, guess PA; sets
+                          // the failure mask, counted only into Ctl::diffuse_err
 };
 
 // Device control block of one solver (one per handle, in device memory).
@@ -72,6 +74,11 @@ struct Ctl {
   int ctu_err[4];
   int ctu_c2p_err;
   int ctu_reset;
+  // GodunovOperator's FailureMask (Mara/hydro.cpp:133-149): one byte per guarded zone, set by
+  // every counted c2p to whether the zone failed (0 after an emergency reset), read by
+  // Mara.diffuse; nullptr where the solver keeps no mask (lean layout, ensembles)
+  unsigned char *fmask;
+  int diffuse_err;                      // failed zones of the last Mara.diffuse c2p
   // since the solver was created (never reset by an advance): advances run, advances not
   // committed, and the failed zones those reported (as Mara.advance returns them)
   unsigned long long n_advances, n_failed, n_failed_zones;
@@ -297,5 +304,6 @@ struct EnsembleArgs {
   cudaError_t face_io_##suffix(const TransferArgs &A, double *d_aos, long long z0, long long count, int to_aos); \
   cudaError_t halo_##suffix(const TransferArgs &A, int which, int dim, int side, void *buf, int pack);   \
   cudaError_t ensemble_advance_##suffix(const EnsembleArgs &E);                                          \
+  cudaError_t diffuse_##suffix(const AdvanceArgs &A, double r);                                          \
   }
 

@@ -28,6 +28,9 @@ struct mgpu_solver {
   long long staging_zones = 0;
   double *red = nullptr;        // reduction partials (device)
   double *red_host = nullptr;   // pinned
+  double *meas = nullptr;       // per-block partials of the measures (device)
+  double *meas_host = nullptr;  // pinned
+  unsigned char *fmask = nullptr;   // failure mask of the last c2p (device, guarded zones)
   float *mlp = nullptr;         // learned c2p network (device)
   long long mlp_count = 0;
   void *mlp_tc = nullptr;       // its tensor-core image (device)

@@ -7,8 +7,11 @@
  *   start, close, set_fluid('rmhd'), set_eos('gamma-law', G), set_boundary('periodic'),
  *   set_godunov('plm-split' | 'plm-muscl'), set_riemann, set_advance, config_solver{...}[, quiet],
  *   set_domain(x0, x1, N, Nq, Ng), init_prim(buf, f), set_primitive(buf),
- *   advance(buf, dt) -> kzps, errors, get_timestep(CFL) -> dt,
- *   measure.mean_max_divB(), measure.max_lorentz_factor(), fluid.GetPrimNames()
+ *   advance(buf, dt) -> kzps, errors, get_timestep(CFL) -> dt, diffuse(buf, r),
+ *   set_failmask(v), cooling_rate(dt) (0: no cooling module), measure.mean_max_divB(),
+ *   measure.max_lorentz_factor(), measure.mean_cons/mean_prim/mean_energies/mean_velocity/
+ *   mean_max_temperature/mean_max_magnetic_field/mean_max_sonic_mach/mean_min_alfvenic_mach(),
+ *   fluid.GetPrimNames()
  *
  * with the reference's argument conventions and error messages (luaL_error for misuse,
  * an error count for numerical failure with the buffer left unchanged).  Entry points of
@@ -23,9 +26,10 @@
  * device-resident state without the per-step host copies of Mara.advance(buf, dt).
  *
  * The solver is one module-level object, as the reference's is (mara.cpp:135).  Scheme
- * changes after set_domain rebuild the device solver at its next use (the state lives in
- * the caller's buffer between advances, so nothing is lost but MaxLambda and the measured
- * array, which the rebuilt solver starts without).
+ * changes after set_domain are applied to the device solver in place at its next use
+ * (mgpu_reconfigure: MaxLambda, the failure mask and the measured array carry over, as in
+ * the reference); only a change of precision or layout rebuilds it, and the rebuilt solver
+ * starts without those.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -75,6 +79,15 @@ static mgpu_solver *solver(lua_State *L)
   if (!M.started) luaL_error(L, "[Mara] call Mara.start() first");
   if (!M.have_domain) luaL_error(L, "[Mara] need a domain to run this, use set_domain");
   if (M.h && !M.dirty) return M.h;
+  if (M.h) {   /* a scheme change: in place where the solver allows it (state, MaxLambda,
+                  failure mask and measured array carry over, as in the reference) */
+    mgpu_config cfg = M.cfg;
+    if (cfg.godunov == MGPU_GODUNOV_PLM_MUSCL) cfg.theta = ctu_theta;
+    if (mgpu_reconfigure(M.h, &cfg) == 0) {
+      M.dirty = 0;
+      return M.h;
+    }
+  }
   if (M.h) {   /* keep the driving field (its OU state) across the rebuild */
     long long n = 0;
     free(M.drive);
@@ -650,6 +663,99 @@ static int l_max_lorentz_factor(lua_State *L)
   return 1;
 }
 
+static int push_array(lua_State *L, const double *a, int n)   /* luaU_pusharray, mara.cpp:1882 */
+{
+  lua_newtable(L);
+  for (int i = 0; i < n; ++i) {
+    lua_pushnumber(L, a[i]);
+    lua_rawseti(L, -2, i + 1);
+  }
+  return 1;
+}
+
+static int l_mean_cons(lua_State *L)
+{
+  double a[8];
+  const int rc = mgpu_measure_mean_cons(solver(L), a);
+  if (rc) return raise_abi(L, rc, "mean_cons");
+  return push_array(L, a, 8);
+}
+
+static int l_mean_prim(lua_State *L)
+{
+  double a[8];
+  const int rc = mgpu_measure_mean_prim(solver(L), a);
+  if (rc) return raise_abi(L, rc, "mean_prim");
+  return push_array(L, a, 8);
+}
+
+static int l_mean_velocity(lua_State *L)
+{
+  double a[4];
+  const int rc = mgpu_measure_mean_velocity(solver(L), a);
+  if (rc) return raise_abi(L, rc, "mean_velocity");
+  return push_array(L, a, 4);
+}
+
+static int l_mean_energies(lua_State *L)   /* a table keyed as luaC_mean_energies' */
+{
+  double a[4];
+  const int rc = mgpu_measure_mean_energies(solver(L), a);
+  if (rc) return raise_abi(L, rc, "mean_energies");
+  lua_newtable(L);
+  lua_pushstring(L, "magnetic"); lua_pushnumber(L, a[0]); lua_settable(L, -3);
+  lua_pushstring(L, "kinetic");  lua_pushnumber(L, a[1]); lua_settable(L, -3);
+  lua_pushstring(L, "internal"); lua_pushnumber(L, a[2]); lua_settable(L, -3);
+  lua_pushstring(L, "total");    lua_pushnumber(L, a[3]); lua_settable(L, -3);
+  return 1;
+}
+
+#define MEAN_EXTREME(fn, api, name)                    \
+  static int fn(lua_State *L)                          \
+  {                                                    \
+    double a = 0.0, b = 0.0;                           \
+    const int rc = api(solver(L), &a, &b);             \
+    if (rc) return raise_abi(L, rc, name);             \
+    lua_pushnumber(L, a);                              \
+    lua_pushnumber(L, b);                              \
+    return 2;                                          \
+  }
+MEAN_EXTREME(l_mean_max_temperature, mgpu_measure_mean_max_temperature, "mean_max_temperature")
+MEAN_EXTREME(l_mean_max_magnetic_field, mgpu_measure_mean_max_magnetic_field, "mean_max_magnetic_field")
+MEAN_EXTREME(l_mean_max_sonic_mach, mgpu_measure_mean_max_sonic_mach, "mean_max_sonic_mach")
+MEAN_EXTREME(l_mean_min_alfvenic_mach, mgpu_measure_mean_min_alfvenic_mach, "mean_min_alfvenic_mach")
+#undef MEAN_EXTREME
+
+/* luaC_Mara_diffuse (mara.cpp:343-366): Mara.diffuse(P, r), P changed in place */
+static int l_diffuse(lua_State *L)
+{
+  double *P = check_prim_buffer(L, 1);
+  const double r = luaL_checknumber(L, 2);
+  int err = 0;
+  const int rc = mgpu_diffuse_host(solver(L), P, r, &err);
+  if (rc) return raise_abi(L, rc, "diffuse");
+  return 0;
+}
+
+/* luaC_Mara_set_failmask (mara.cpp:368-373) */
+static int l_set_failmask(lua_State *L)
+{
+  const int value = (int) luaL_checkinteger(L, 1);
+  printf("[Mara] set fail mask value everywhere to %d\n", value);
+  const int rc = mgpu_set_failmask(solver(L), value);
+  if (rc) return raise_abi(L, rc, "set_failmask");
+  return 0;
+}
+
+/* luaC_cooling_rate (mara.cpp:1296-1308): the GPU module has no cooling (set_cooling is not
+ * provided), so the rate is the reference's value without a cooling module, 0. */
+static int l_cooling_rate(lua_State *L)
+{
+  (void) luaL_checknumber(L, 1);
+  lua_pushnumber(L, 0.0);
+  return 1;
+}
+
 /* ---- Mara.fluid.* ------------------------------------------------------------------------ */
 
 static int l_GetPrimNames(lua_State *L)
@@ -703,17 +809,26 @@ int luaopen_Mara(lua_State *L)
       {"upload_primitive", l_upload_primitive},
       {"advance_device", l_advance_device},
       {"download_primitive", l_download_primitive},
+      {"diffuse", l_diffuse},
+      {"set_failmask", l_set_failmask},
+      {"cooling_rate", l_cooling_rate},
       {NULL, NULL}};
-  static const char *const absent[] = {"show", "diffuse", "set_failmask", "prim_at_point", "set_units",
+  static const char *const absent[] = {"show", "prim_at_point", "set_units",
                                        "set_cooling", "set_fluxsrc", "set_srcterm",
-                                       "cooling_rate", "load_shen", "test_shen",
+                                       "load_shen", "test_shen",
                                        "test_rmhd_c2p", "test_sampling", "test_sampling_many", NULL};
   static const luaL_Reg measure[] = {{"mean_max_divB", l_mean_max_divB},
                                      {"max_lorentz_factor", l_max_lorentz_factor},
+                                     {"mean_cons", l_mean_cons},
+                                     {"mean_prim", l_mean_prim},
+                                     {"mean_energies", l_mean_energies},
+                                     {"mean_velocity", l_mean_velocity},
+                                     {"mean_max_temperature", l_mean_max_temperature},
+                                     {"mean_max_magnetic_field", l_mean_max_magnetic_field},
+                                     {"mean_max_sonic_mach", l_mean_max_sonic_mach},
+                                     {"mean_min_alfvenic_mach", l_mean_min_alfvenic_mach},
                                      {NULL, NULL}};
-  static const char *const measure_absent[] = {"mean_cons", "mean_prim", "mean_energies", "mean_velocity",
-                                               "mean_max_temperature", "mean_max_sonic_mach",
-                                               "mean_min_alfvenic_mach", "mean_max_magnetic_field", NULL};
+  static const char *const measure_absent[] = {NULL};
   static const luaL_Reg fluid[] = {{"GetPrimNames", l_GetPrimNames}, {NULL, NULL}};
   static const char *const fluid_absent[] = {"PrimToCons", "ConsToPrim", "Eigensystem", "FluxFunction", NULL};
 

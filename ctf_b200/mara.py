@@ -218,6 +218,66 @@ class Solver:
         self._check(self.lib.mgpu_max_lorentz_factor(self.h, ctypes.byref(w)))
         return w.value
 
+    # ---- the other Mara.measure.* (Mara/mara.cpp:1954-2230), on the measured array -----------
+    def _vec(self, fn, n):
+        out = (ctypes.c_double * n)()
+        self._check(fn(self.h, out))
+        return list(out)
+
+    def _pair(self, fn):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(fn(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def mean_cons(self) -> list:
+        return self._vec(self.lib.mgpu_measure_mean_cons, 8)
+
+    def mean_prim(self) -> list:
+        return self._vec(self.lib.mgpu_measure_mean_prim, 8)
+
+    def mean_energies(self) -> dict:
+        e = self._vec(self.lib.mgpu_measure_mean_energies, 4)
+        return dict(zip(("magnetic", "kinetic", "internal", "total"), e))
+
+    def mean_velocity(self) -> list:
+        return self._vec(self.lib.mgpu_measure_mean_velocity, 4)
+
+    def mean_max_temperature(self):
+        return self._pair(self.lib.mgpu_measure_mean_max_temperature)
+
+    def mean_max_magnetic_field(self):
+        return self._pair(self.lib.mgpu_measure_mean_max_magnetic_field)
+
+    def mean_max_sonic_mach(self):
+        return self._pair(self.lib.mgpu_measure_mean_max_sonic_mach)
+
+    def mean_min_alfvenic_mach(self):
+        return self._pair(self.lib.mgpu_measure_mean_min_alfvenic_mach)
+
+    # ---- Mara.diffuse / set_failmask, scheme changes in place -------------------------------
+    def diffuse(self, r: float) -> int:
+        """LaxDiffusion of strength r around the zones that failed the last c2p, on the
+        committed state; returns the failed zones of its c2p."""
+        e = ctypes.c_int()
+        self._check(self.lib.mgpu_diffuse(self.h, ctypes.c_double(r), ctypes.byref(e)))
+        return e.value
+
+    def diffuse_host(self, P: np.ndarray, r: float) -> int:
+        """Mara.diffuse(P, r): P is copied in, diffused and copied back."""
+        self._check_buf(P)
+        e = ctypes.c_int()
+        self._check(self.lib.mgpu_diffuse_host(self.h, _dp(P), ctypes.c_double(r), ctypes.byref(e)))
+        return e.value
+
+    def set_failmask(self, value: int):
+        self._check(self.lib.mgpu_set_failmask(self.h, int(value)))
+
+    def reconfigure(self, scheme: "Scheme"):
+        """Change the scheme in place (state, MaxLambda, failure mask and measured array kept)."""
+        cfg = scheme.to_config()
+        self._check(self.lib.mgpu_reconfigure(self.h, ctypes.byref(cfg)))
+        self.scheme = scheme
+
     KERNEL_CLASSES = ["begin", "p2c", "c2p", "flux", "update", "predict"]
 
     def profile_enable(self, capacity: int = 4096):
@@ -290,6 +350,30 @@ class _Measure:
     def max_lorentz_factor(self):
         return self._m._solver().max_lorentz_factor()
 
+    def mean_cons(self):
+        return self._m._solver().mean_cons()
+
+    def mean_prim(self):
+        return self._m._solver().mean_prim()
+
+    def mean_energies(self):
+        return self._m._solver().mean_energies()
+
+    def mean_velocity(self):
+        return self._m._solver().mean_velocity()
+
+    def mean_max_temperature(self):
+        return self._m._solver().mean_max_temperature()
+
+    def mean_max_magnetic_field(self):
+        return self._m._solver().mean_max_magnetic_field()
+
+    def mean_max_sonic_mach(self):
+        return self._m._solver().mean_max_sonic_mach()
+
+    def mean_min_alfvenic_mach(self):
+        return self._m._solver().mean_min_alfvenic_mach()
+
 
 class _Fluid:
     def __init__(self, mod):
@@ -318,6 +402,7 @@ class MaraModule:
         self._godunov = None
         self._domain = None
         self._s = None
+        self._dirty = False
         self._started = False
 
     # lifecycle ---------------------------------------------------------------------------
@@ -337,6 +422,12 @@ class MaraModule:
             raise MaraError("[Mara] call Mara.start() first")
 
     def _invalidate(self):
+        """A scheme change: applied to the solver in place at its next use (so MaxLambda,
+        the failure mask and the measured array carry over, as in the reference's
+        process-wide solver), or by a new solver where the change needs one."""
+        self._dirty = True
+
+    def _rebuild(self):
         if self._s is not None:
             self._s.close()
             self._s = None
@@ -348,7 +439,7 @@ class MaraModule:
             raise MaraError(f"[Mara] no such fluid '{key}'" if key not in ("euler", "srhd")
                             else f"[Mara] fluid '{key}' is not provided by the B200 module")
         self._fluid = key
-        self._invalidate()
+        self._rebuild()
 
     def set_eos(self, key: str, gamma: float = 1.4):
         self._need_start()
@@ -435,16 +526,22 @@ class MaraModule:
         if Nq != 8:
             raise MaraError("[Mara] the rmhd fluid has Nq = 8")
         self._domain = (tuple(x0), tuple(x1), tuple(int(v) for v in N), int(Ng))
-        self._invalidate()
+        self._rebuild()
 
     def _solver(self) -> Solver:
         if self._domain is None:
             raise MaraError("[Mara] need a domain to run this, use set_domain")
+        scheme = replace(self._scheme, godunov=self._godunov or "plm-split")
+        if scheme.godunov == "plm-muscl":
+            scheme.theta = MaraModule._ctu_theta
+        if self._s is not None and self._dirty:
+            try:
+                self._s.reconfigure(scheme)
+            except MaraError:
+                self._rebuild()
+        self._dirty = False
         if self._s is None:
             x0, x1, N, Ng = self._domain
-            scheme = replace(self._scheme, godunov=self._godunov or "plm-split")
-            if scheme.godunov == "plm-muscl":
-                scheme.theta = MaraModule._ctu_theta
             self._s = Solver(scheme, N, x0, x1, Ng)
         return self._s
 
@@ -476,6 +573,15 @@ class MaraModule:
 
     def get_timestep(self, cfl: float) -> float:
         return self._solver().get_timestep(cfl)
+
+    def diffuse(self, P: np.ndarray, r: float):
+        """luaC_Mara_diffuse (Mara/mara.cpp:343-366): P gets Lax diffusion of strength r
+        around the zones that failed the last c2p (in place)."""
+        self._solver().diffuse_host(P, r)
+
+    def set_failmask(self, value: int):
+        """luaC_Mara_set_failmask (Mara/mara.cpp:368-373)."""
+        self._solver().set_failmask(value)
 
 
 Mara = MaraModule()

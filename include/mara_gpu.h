@@ -149,6 +149,48 @@ int mgpu_max_lorentz_factor(mgpu_solver *h, double *wmax);
  * precisions (the FP32-bulk path keeps B, its CT update and ∇·B in FP64). */
 int mgpu_measure_divB_state(mgpu_solver *h, double *mean, double *max);
 
+/* The other measures of Mara.measure (Mara/mara.cpp:1954-2230), on the same measured
+ * primitive array as mgpu_measure_divB: means over the interior zones (sums divided by the
+ * global interior zone count, as the reference's TTL_ZONES), extremes over them.  Units are
+ * the reference's default PhysicalUnits(1, 1, 1) (Mara/hydro.cpp:20).  One device pass per
+ * call; each per-zone value in the reference's operation order, the sums in another order.
+ *   mean_cons       out[8]  mean of P->U                      (luaC_mean_cons)
+ *   mean_prim       out[8]  mean of the primitives            (luaC_mean_prim)
+ *   mean_energies   out[4]  magnetic, kinetic, internal, total (luaC_mean_energies)
+ *   mean_velocity   out[4]  mean W, |vx|, |vy|, |vz|          (luaC_mean_velocity)
+ *   mean_max_temperature     mean, max of T in MeV            (luaC_mean_max_temperature)
+ *   mean_max_magnetic_field  mean, max of |B| in Gauss        (luaC_mean_max_magnetic_field)
+ *   mean_max_sonic_mach      mean, max of the sonic Mach number (luaC_mean_max_sonic_mach)
+ *   mean_min_alfvenic_mach   mean, min of the Alfvenic Mach number (luaC_mean_min_alfvenic_mach) */
+int mgpu_measure_mean_cons(mgpu_solver *h, double *out);
+int mgpu_measure_mean_prim(mgpu_solver *h, double *out);
+int mgpu_measure_mean_energies(mgpu_solver *h, double *out);
+int mgpu_measure_mean_velocity(mgpu_solver *h, double *out);
+int mgpu_measure_mean_max_temperature(mgpu_solver *h, double *mean, double *max);
+int mgpu_measure_mean_max_magnetic_field(mgpu_solver *h, double *mean, double *max);
+int mgpu_measure_mean_max_sonic_mach(mgpu_solver *h, double *mean, double *max);
+int mgpu_measure_mean_min_alfvenic_mach(mgpu_solver *h, double *mean, double *min);
+
+/* replaces luaC_Mara_diffuse (Mara/mara.cpp:343-366): the committed state becomes c2p of
+ * P->U(P) + GodunovOperator::LaxDiffusion(U, r) (Mara/hydro.cpp:205-283) -- Lax-Friedrichs
+ * fluxes of strength r on the faces next to zones that failed the last c2p (the failure mask
+ * of the last advance or diffuse, or of mgpu_set_failmask), with flux-CT -- with the measured
+ * primitive array as the c2p's previous state; that array is left unchanged and the mask
+ * becomes this c2p's.  *errors = the failed zones of that c2p (the reference discards the
+ * count).  Standard layout, single domain.  Synchronous. */
+int mgpu_diffuse(mgpu_solver *h, double r, int *errors);
+/* Mara.diffuse(buf, r) exactly: the host buffer is copied in, diffused and copied back. */
+int mgpu_diffuse_host(mgpu_solver *h, double *host_aos, double r, int *errors);
+/* replaces luaC_Mara_set_failmask (Mara/mara.cpp:368-373): every zone's mask entry = value. */
+int mgpu_set_failmask(mgpu_solver *h, int value);
+/* Changes the scheme of a solver in place (the set_riemann / set_advance / set_godunov /
+ * config_solver calls of the reference's crash ladders, e.g. ctf-core/drvtrb.lua:276-352),
+ * keeping its state, MaxLambda, failure mask, measured array and driving field, as the
+ * reference's process-wide solver keeps them.  The fluid, precision and layout cannot change
+ * (MGPU_ERR_UNSUPPORTED: create a new solver); arrays the new scheme needs (RK4 registers,
+ * CTU-Hancock predictions) are allocated here. */
+int mgpu_reconfigure(mgpu_solver *h, const mgpu_config *cfg);
+
 /* Kernel timing (no counterpart in the reference): while enabled, every kernel launch of an
  * advance is bracketed by CUDA events on the handle's stream.  Classes (MGPU_KERNEL_CLASSES):
  * 0 begin/commit, 1 P->U, 2 c2p, 3 flux sweep, 4 CT+divergence+RK update, 5 CTU-Hancock
@@ -230,6 +272,40 @@ int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult);  
 int mgpu_halo_bytes(mgpu_solver *h, int which, int dim, long long *bytes);
 int mgpu_halo_pack(mgpu_solver *h, int which, int dim, int side, void *dev_buf);
 int mgpu_halo_unpack(mgpu_solver *h, int which, int dim, int side, const void *dev_buf);
+
+/* ---- function-level probes (test infrastructure of the parity suite; no counterpart in
+ * the reference's Lua API).  Each applies one FP64 device function of the advance to n
+ * independent states held in device memory (AoS, 8 doubles per state) and returns after the
+ * work is done; each replaces, for per-function comparison, the reference function named:
+ *   mgpu_probe_prim_to_cons  AdiabaticIdealRmhd::PrimToCons (Mara/rmhd.cpp:177-207); err =
+ *                            its check of the conserved state.
+ *   mgpu_probe_c2p           mode 0: AdiabaticIdealRmhd::ConsToPrim, the gamma-law ladder
+ *                            (Mara/rmhd.cpp:103-176) with dev_guess as the previous primitives
+ *                            (dev_P = dev_guess where it fails); mode 1 + 2*solver + start: one
+ *                            solver, rmhd_c2p_solve_anton2dzw (solver 0) or _noble1dw (1)
+ *                            (Mara/rmhd-c2p.c:182-326), started from rmhd_c2p_estimate_from_cons
+ *                            (start 0) or rmhd_c2p_set_starting_prim(dev_guess) (start 1)
+ *                            (Mara/rmhd-c2p.c:96-119); iters = Newton iterations.
+ *   mgpu_probe_flux          FluxAndEigenvalues (Mara/rmhd.cpp:208-310) of P->U(P) in
+ *                            direction dim: dev_F n x 8, dev_lam n x 2 (lambda+, lambda-).
+ *   mgpu_probe_riemann       IntercellFlux at s = 0 of MGPU_RIEMANN_HLL / HLLC / HLLD
+ *                            (Mara/riemann_hll.cpp:19-64, riemann_hllc-rmhd.cpp:26-178,
+ *                            riemann_hlld-rmhd.cpp:143-277) on face pairs in direction dim, or
+ *                            per face dev_dims[i] when dev_dims is not NULL; dev_max_lambda[i]
+ *                            = RiemannSolver::MaxLambda after that face alone; dev_used_hllc
+ *                            (may be NULL) = 1 where HLLD fell back to HLLC.
+ *   mgpu_probe_reconstruct   reconstruct (Mara/weno.c:58-154) on stencils dev_V (n x 5, centre
+ *                            at 2): op 0 / 1 PLM minmod(theta) left / right face, op 4 / 5
+ *                            WENO5 FV centre-to-right / centre-to-left (is_mode, sz10A). */
+int mgpu_probe_prim_to_cons(double gamma, const double *dev_P, long long n, double *dev_U, int *dev_err);
+int mgpu_probe_c2p(int mode, double gamma, double pfloor, const double *dev_U, const double *dev_guess, long long n,
+                   double *dev_P, int *dev_err, int *dev_iters);
+int mgpu_probe_flux(double gamma, int dim, const double *dev_P, long long n, double *dev_F, double *dev_lam);
+int mgpu_probe_riemann(int riemann, int dim, const int *dev_dims, double gamma, double pfloor, const double *dev_Pl,
+                       const double *dev_Pr, long long n, double *dev_F, int *dev_err, double *dev_max_lambda,
+                       int *dev_used_hllc);
+int mgpu_probe_reconstruct(int op, double theta, int is_mode, double sz10A, const double *dev_V, long long n,
+                           double *dev_out);
 
 /* Allocation-free advance (no counterpart in the reference).  For callers that may not
  * allocate device memory -- allocation-free sections of a larger application, real-time

@@ -86,7 +86,7 @@ class _PortConfig(ctypes.Structure):
 
 class _PortStats(ctypes.Structure):
     _fields_ = [("max_lambda", ctypes.c_double), ("hlld_success", ctypes.c_long),
-                ("hlld_failure", ctypes.c_long)]
+                ("hlld_failure", ctypes.c_long), ("hlld_path", ctypes.c_int)]
 
 
 class PortOracle:
@@ -149,6 +149,30 @@ class PortOracle:
 
     def max_lorentz_factor(self, prim: np.ndarray) -> float:
         return self.lib.port_max_lorentz_factor(ctypes.byref(self.cfg), _p(prim))
+
+    MEASURES = {"mean_cons": (0, 8), "mean_prim": (8, 8), "mean_energies": (16, 4), "mean_velocity": (20, 4),
+                "mean_max_temperature": (24, 2), "mean_max_magnetic_field": (26, 2),
+                "mean_max_sonic_mach": (28, 2), "mean_min_alfvenic_mach": (30, 2)}
+
+    def measure(self, name: str, prim: np.ndarray) -> list:
+        """The measure `name` of Mara.measure on the interior zones of prim (as RefOracle.measure
+        returns it)."""
+        out = np.zeros(32)
+        self.lib.port_measures(ctypes.byref(self.cfg), _p(np.ascontiguousarray(prim)), _p(out))
+        a, n = self.MEASURES[name]
+        return list(out[a:a + n])
+
+    def diffuse(self, prim: np.ndarray, r: float, mask: np.ndarray, prev: np.ndarray):
+        """Mara.diffuse(P, r) given the FailureMask and PrimitiveArray it reads; prim changes in
+        place; returns the new mask and the c2p's failure count."""
+        assert prim.dtype == np.float64 and prim.flags.c_contiguous
+        m_in = np.ascontiguousarray(mask, dtype=np.int32).ravel()
+        m_out = np.zeros_like(m_in)
+        pv = np.ascontiguousarray(prev, dtype=np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        e = self.lib.port_diffuse(ctypes.byref(self.cfg), _p(prim), ctypes.c_double(r),
+                                  m_in.ctypes.data_as(ip), _p(pv), m_out.ctypes.data_as(ip))
+        return m_out, e
 
     # per state ----------------------------------------------------------------------
     def prim_to_cons(self, P):
@@ -213,6 +237,8 @@ class RefOracle:
         L.ref_last_error.restype = ctypes.c_char_p
         L.ref_get_max_lambda.restype = ctypes.c_double
         L.ref_reconstruct.restype = ctypes.c_double
+        L.ref_failure_mask.restype = ctypes.c_long
+        L.ref_primitive_array.restype = ctypes.c_long
         self.scheme = s = scheme
         L.ref_open()
         lua = (f"Mara.start(); Mara.set_fluid('rmhd'); Mara.set_eos('gamma-law', {s.gamma!r}); "
@@ -290,6 +316,41 @@ class RefOracle:
         w = ctypes.c_double()
         self.lib.ref_max_lorentz_factor(ctypes.byref(w))
         return w.value
+
+    def diffuse(self, prim: np.ndarray, r: float):
+        """Mara.diffuse(P, r) (Mara/mara.cpp:343-366), P changed in place."""
+        assert prim.dtype == np.float64 and prim.flags.c_contiguous
+        if self.lib.ref_diffuse(_p(prim), ctypes.c_long(prim.size), ctypes.c_double(r)):
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def set_failmask(self, value: int):
+        self.dostring(f"Mara.set_failmask({int(value)})")
+
+    def measure(self, name: str, prim: np.ndarray | None = None) -> list:
+        """Mara.measure.<name>() on the reference's PrimitiveArray (set to `prim` first when
+        given): its numbers, array entries, or mean_energies' magnetic, kinetic, internal,
+        total."""
+        if prim is not None:
+            self.set_primitive(prim)
+        out = (ctypes.c_double * 8)()
+        n = ctypes.c_int()
+        if self.lib.ref_measure(name.encode(), out, 8, ctypes.byref(n)):
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return list(out[:n.value])
+
+    def failure_mask(self) -> np.ndarray:
+        """GodunovOperator's FailureMask, one entry per guarded zone."""
+        n = int(np.prod(self.scheme.shape))
+        out = np.zeros(n, dtype=np.int32)
+        k = self.lib.ref_failure_mask(out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.c_long(n))
+        return out[:k]
+
+    def primitive_array(self) -> np.ndarray:
+        """The application's PrimitiveArray (what the next Mara.diffuse reads as its guess)."""
+        n = int(np.prod(self.scheme.shape)) * 8
+        out = np.zeros(n)
+        k = self.lib.ref_primitive_array(_p(out), ctypes.c_long(n))
+        return out[:k]
 
     def prim_to_cons(self, P):
         P = np.ascontiguousarray(P, dtype=np.float64)

@@ -924,6 +924,7 @@ static int riemann_hlld(const port_config *c, port_stats *st, const double *pl,
     success = (rc == 0);
     ++attempt;
   }
+  st->hlld_path = hll_c2p_failed ? 0 : success ? attempt : 4;
   if (success) {
     st->hlld_success++;
     f[ddd] = F[ddd];
@@ -1059,7 +1060,16 @@ static void sync_periodic(const port_config *c, const grid_t *g, double *A)
 
 /* GodunovOperator::ConsToPrim (Mara/hydro.cpp:125-202), with the emergency reset.
  * U is ghost-filled in place; P holds the previous prims (guess) and is overwritten. */
+static int c2p_all_mask(const port_config *c, const grid_t *g, double *U, double *P, int *mask_out);
+
 static int c2p_all(const port_config *c, const grid_t *g, double *U, double *P)
+{
+  return c2p_all_mask(c, g, U, P, NULL);
+}
+
+/* ... and GodunovOperator's FailureMask afterwards (zeroed by an emergency reset) in mask_out
+ * when it is not NULL. */
+static int c2p_all_mask(const port_config *c, const grid_t *g, double *U, double *P, int *mask_out)
 {
   sync_periodic(c, g, U);
   int ttl = 0;
@@ -1082,7 +1092,10 @@ static int c2p_all(const port_config *c, const grid_t *g, double *U, double *P)
     }
     for (long z = 0; z < g->nz; ++z) port_prim_to_cons(c, &P[z * 8], &U[z * 8]);
     ttl = 0;
+    memset(mask, 0, g->nz);
   }
+  if (mask_out)
+    for (long z = 0; z < g->nz; ++z) mask_out[z] = mask[z];
   free(mask);
   return ttl;
 }
@@ -1417,4 +1430,168 @@ double port_max_lorentz_factor(const port_config *c, const double *P)
         if (W0 > mx) mx = W0;
       }
   return mx;
+}
+
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* luaC_Mara_diffuse (Mara/mara.cpp:343-366) with GodunovOperator::LaxDiffusion
+ * (Mara/hydro.cpp:205-283): prim <- c2p(P->U(prim) + L), L the CT'd divergence of the
+ * Lax fluxes -c r (U[i+s] - U[i]) dx_d on faces with a failed zone (mask_in, one entry per
+ * guarded zone) on either side.  prev = the PrimitiveArray the c2p starts from and keeps in
+ * failed zones; mask_out = the FailureMask after (may alias mask_in).  Returns the c2p's
+ * failure count, which the reference discards. */
+int port_diffuse(const port_config *c, double *prim, double r, const int *mask_in, const double *prev,
+                 int *mask_out)
+{
+  grid_t g;
+  grid_init(c, &g);
+  const long n = g.nz * 8;
+  const int nd = c->nd, NQ = 8;
+  double *P = malloc(n * sizeof(double)), *U = malloc(n * sizeof(double));
+  double *L = calloc(n, sizeof(double));
+  double *Fiph = calloc(n, sizeof(double)), *Giph = calloc(n, sizeof(double));
+  double *Hiph = calloc(n, sizeof(double));
+  int *FM = malloc(g.nz * sizeof(int));
+  for (long z = 0; z < g.nz; ++z) FM[z] = mask_in[z];
+  memcpy(P, prim, n * sizeof(double));
+  sync_periodic(c, &g, P);                                  /* GodunovOperator::PrimToCons */
+  for (long z = 0; z < g.nz; ++z) port_prim_to_cons(c, &P[z * 8], &U[z * 8]);
+  sync_periodic(c, &g, U);                                  /* LaxDiffusion: ApplyBoundaries(U) */
+  const int Ni = g.stride[0], sx = g.stride[1], sy = g.stride[2], sz = g.stride[3];
+  if (nd == 1) {
+    for (int i = 0; i < Ni - sx; i += NQ)
+      if (FM[i / NQ] || FM[(i + sx) / NQ])
+        for (int j = 0; j < NQ; ++j) Fiph[i + j] = -0.5 * r * (U[i + j + sx] - U[i + j]) * g.dx;
+    for (int i = sx; i < Ni - sx; ++i) L[i] = -((Fiph[i] - Fiph[i - sx]) / g.dx);
+  } else if (nd == 2) {
+    for (int i = 0; i < Ni - sx; i += NQ) {
+      if (FM[i / NQ] || FM[(i + sx) / NQ])
+        for (int j = 0; j < NQ; ++j) Fiph[i + j] = -0.25 * r * (U[i + j + sx] - U[i + j]) * g.dx;
+      if (FM[i / NQ] || FM[(i + sy) / NQ])
+        for (int j = 0; j < NQ; ++j) Giph[i + j] = -0.25 * r * (U[i + j + sy] - U[i + j]) * g.dy;
+    }
+    port_ct2d(Fiph, Giph, g.stride);
+    for (int i = sx; i < Ni - sx; ++i)
+      L[i] = -((Fiph[i] - Fiph[i - sx]) / g.dx + (Giph[i] - Giph[i - sy]) / g.dy);
+  } else {
+    for (int i = 0; i < Ni - sx; i += NQ) {
+      if (FM[i / NQ] || FM[(i + sx) / NQ])
+        for (int j = 0; j < NQ; ++j) Fiph[i + j] = -(1.0 / 6.0) * r * (U[i + j + sx] - U[i + j]) * g.dx;
+      if (FM[i / NQ] || FM[(i + sy) / NQ])
+        for (int j = 0; j < NQ; ++j) Giph[i + j] = -(1.0 / 6.0) * r * (U[i + j + sy] - U[i + j]) * g.dy;
+      if (FM[i / NQ] || FM[(i + sz) / NQ])
+        for (int j = 0; j < NQ; ++j) Hiph[i + j] = -(1.0 / 6.0) * r * (U[i + j + sz] - U[i + j]) * g.dz;
+    }
+    port_ct3d(Fiph, Giph, Hiph, g.stride);
+    for (int i = sx; i < Ni - sx; ++i)
+      L[i] = -((Fiph[i] - Fiph[i - sx]) / g.dx + (Giph[i] - Giph[i - sy]) / g.dy + (Hiph[i] - Hiph[i - sz]) / g.dz);
+  }
+  for (long i = 0; i < n; ++i) U[i] += L[i];
+  memcpy(P, prev, n * sizeof(double));                      /* P = Mara->PrimitiveArray */
+  const int err = c2p_all_mask(c, &g, U, P, FM);
+  memcpy(prim, P, n * sizeof(double));
+  for (long z = 0; z < g.nz; ++z) mask_out[z] = FM[z];
+  free(P); free(U); free(L); free(Fiph); free(Giph); free(Hiph); free(FM);
+  return err;
+}
+
+/* The eight other measures of Mara.measure (Mara/mara.cpp:1954-2230) on the interior zones of
+ * P, in the cgs units of a started reference (PhysicalUnits(1, 1, 1), Mara/hydro.cpp:20):
+ * out[0..7] mean_cons, [8..15] mean_prim, [16..19] mean_energies (magnetic, kinetic, internal,
+ * total), [20..23] mean_velocity, [24, 25] mean_max_temperature, [26, 27]
+ * mean_max_magnetic_field, [28, 29] mean_max_sonic_mach, [30, 31] mean_min_alfvenic_mach. */
+void port_measures(const port_config *c, const double *P, double *out)
+{
+  int G[3];
+  shape(c, G);
+  const double Gamma = c->gamma;
+  /* PhysicalUnits (Mara/units.cpp) at Length = Mass = Time = 1 */
+  const double gram = 1.0 / 1.0, cm = 1.0 / 1.0, sec = 1.0 / 1.0;
+  const double erg = gram * pow(cm / sec, 2.0);
+  const double erg_cc = 1.60217648740e-06 * erg / pow(1e-13 * cm, 3) * 1e-33;
+  const double g_cc = gram / pow(cm, 3.0);
+  const double mp = 1.67262177774e-24 * gram, kb = 1.38064881300e-16 * erg;
+  const double gauss = sqrt(erg / pow(cm, 3.0) / (4 * M_PI));
+  double U[8], sumU[8] = {0}, sumP[8] = {0}, Vrms[4] = {0};
+  double kinetic = 0, internal = 0, magnetic = 0, total = 0;
+  double tT = 0, mT = 0, tMs = 0, mMs = 0, tMa = 0, mMa = 1e20, tB = 0, mB = 0;
+  for (int i = 0; i < G[0]; ++i)
+    for (int j = 0; j < G[1]; ++j)
+      for (int k = 0; k < G[2]; ++k) {
+        if (i < c->ng || i >= G[0] - c->ng) continue;
+        if (c->nd >= 2 && (j < c->ng || j >= G[1] - c->ng)) continue;
+        if (c->nd >= 3 && (k < c->ng || k >= G[2] - c->ng)) continue;
+        const double *P0 = &P[(((long) i * G[1] + j) * G[2] + k) * 8];
+        port_prim_to_cons(c, P0, U);
+        for (int q = 0; q < 8; ++q) {
+          sumU[q] += U[q];
+          sumP[q] += P0[q];
+        }
+        const double v2 = P0[2] * P0[2] + P0[3] * P0[3] + P0[4] * P0[4];
+        const double T0 = P0[1];
+        const double u0 = T0 / (Gamma - 1);
+        {
+          const double rhoh = P0[0] + u0 + P0[1];
+          const double W0 = 1.0 / sqrt(1.0 - v2);
+          const double e_f = rhoh * W0 * W0 - P0[1] - U[0];
+          const double e_m = U[1] - e_f;
+          magnetic += e_m;
+          kinetic += P0[0] * W0 * (W0 - 1);
+          internal += W0 * u0;
+          total += U[1];
+        }
+        Vrms[0] += 1.0 / sqrt(1.0 - v2);
+        Vrms[1] += fabs(P0[2]);
+        Vrms[2] += fabs(P0[3]);
+        Vrms[3] += fabs(P0[4]);
+        {
+          const double Pc = P0[1] / erg_cc, rc = P0[0] / g_cc;
+          const double T_K = (Pc / rc) * (mp / kb);
+          const double Tm = T_K * 8.621738e-11;
+          tT += Tm;
+          if (Tm > mT) mT = Tm;
+        }
+        {
+          const double rhoh = P0[0] + T0 / (Gamma - 1) + T0;
+          const double cs2 = Gamma * T0 / rhoh;
+          const double M0 = sqrt((v2 / (1 - v2)) / (cs2 / (1 - cs2)));
+          tMs += M0;
+          if (M0 > mMs) mMs = M0;
+        }
+        {
+          const double B2 = P0[5] * P0[5] + P0[6] * P0[6] + P0[7] * P0[7];
+          const double rhoh = P0[0] + u0 + P0[1];
+          const double va2 = B2 / (B2 + rhoh);
+          const double M0 = sqrt((v2 / (1 - v2)) / (va2 / (1 - va2)));
+          tMa += M0;
+          if (M0 < mMa) mMa = M0;
+        }
+        {
+          const double B0 = sqrt(P0[5] * P0[5] + P0[6] * P0[6] + P0[7] * P0[7]);
+          tB += B0;
+          if (B0 > mB) mB = B0;
+        }
+      }
+  long ttl = 1;
+  for (int d = 0; d < c->nd; ++d) ttl *= c->n[d];
+  for (int q = 0; q < 8; ++q) {
+    out[q] = sumU[q] / ttl;
+    out[8 + q] = sumP[q] / ttl;
+  }
+  out[16] = magnetic / ttl;
+  out[17] = kinetic / ttl;
+  out[18] = internal / ttl;
+  out[19] = total / ttl;
+  for (int q = 0; q < 4; ++q) out[20 + q] = Vrms[q] / ttl;
+  out[24] = tT / ttl;
+  out[25] = mT;
+  out[26] = (1.0 / gauss) * tB / ttl;
+  out[27] = (1.0 / gauss) * mB;
+  out[28] = tMs / ttl;
+  out[29] = mMs;
+  out[30] = tMa / ttl;
+  out[31] = mMa;
 }

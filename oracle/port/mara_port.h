@@ -36,6 +36,9 @@ typedef struct {
   double max_lambda;      /* RiemannSolver::MaxLambda */
   long   hlld_success;    /* HlldRmhdRiemannSolver::NumberOfSuccess */
   long   hlld_failure;    /* HlldRmhdRiemannSolver::NumberOfFailure */
+  int    hlld_path;       /* the last HLLD face (test instrumentation, not in the reference):
+                             1-3 = the attempt whose pressure guess succeeded, 0 = the HLL-state
+                             c2p failed, 4 = all attempts failed (both: HLLC fallback) */
 } port_stats;
 
 void   port_default_config(port_config *c);
@@ -60,6 +63,10 @@ double port_timestep(const port_config *c, double max_lambda, double cfl);
 void   port_mean_max_divB(const port_config *c, const double *prim, double *mean,
                           double *max);
 double port_max_lorentz_factor(const port_config *c, const double *prim);
+
+int    port_diffuse(const port_config *c, double *prim, double r, const int *mask_in, const double *prev,
+                    int *mask_out);
+void   port_measures(const port_config *c, const double *P, double *out);
 
 #ifdef __cplusplus
 }

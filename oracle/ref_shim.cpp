@@ -153,9 +153,96 @@ int ref_max_lorentz_factor(double *w)
   return call_numbers("measure", "max_lorentz_factor", 0, 0, 1, w);
 }
 
+/* Mara.diffuse(buf, r) (Mara/mara.cpp:343-366) on a copy of `prim`, copied back. */
+int ref_diffuse(double *prim, long n, double r)
+{
+  if (!L) return fail("ref_open not called");
+  lua_getglobal(L, "Mara");
+  lua_getfield(L, -1, "diffuse");
+  void *ud = lua_newuserdata(L, n * sizeof(double));
+  memcpy(ud, prim, n * sizeof(double));
+  lua_pushvalue(L, -1);
+  lua_setglobal(L, "__ref_buf");
+  lua_pushnumber(L, r);
+  if (lua_pcall(L, 2, 0, 0)) {
+    last_error = lua_tostring(L, -1);
+    lua_pop(L, 2);
+    return 1;
+  }
+  lua_pop(L, 1);
+  memcpy(prim, ud, n * sizeof(double));
+  lua_pushnil(L);
+  lua_setglobal(L, "__ref_buf");
+  return 0;
+}
+
+int ref_set_failmask(int value)
+{
+  char code[64];
+  snprintf(code, sizeof(code), "Mara.set_failmask(%d)", value);
+  return ref_dostring(code);
+}
+
+/* Mara.measure.<name>() -> up to nmax numbers: the returned numbers, or the entries 1..n of
+ * a returned array table, or (mean_energies) the keys magnetic, kinetic, internal, total. */
+int ref_measure(const char *name, double *out, int nmax, int *nout)
+{
+  if (!L) return fail("ref_open not called");
+  const int top = lua_gettop(L);
+  lua_getglobal(L, "Mara");
+  lua_getfield(L, -1, "measure");
+  lua_getfield(L, -1, name);
+  if (lua_pcall(L, 0, LUA_MULTRET, 0)) {
+    last_error = lua_tostring(L, -1);
+    lua_settop(L, top);
+    return 1;
+  }
+  const int nret = lua_gettop(L) - (top + 2);
+  int n = 0;
+  if (nret == 1 && lua_istable(L, -1)) {
+    if (lua_rawlen(L, -1) > 0) {
+      for (int i = 1; i <= (int) lua_rawlen(L, -1) && n < nmax; ++i) {
+        lua_rawgeti(L, -1, i);
+        out[n++] = lua_tonumber(L, -1);
+        lua_pop(L, 1);
+      }
+    } else {
+      static const char *keys[4] = {"magnetic", "kinetic", "internal", "total"};
+      for (int i = 0; i < 4 && n < nmax; ++i) {
+        lua_getfield(L, -1, keys[i]);
+        out[n++] = lua_tonumber(L, -1);
+        lua_pop(L, 1);
+      }
+    }
+  } else {
+    for (int i = 0; i < nret && n < nmax; ++i) out[n++] = lua_tonumber(L, top + 3 + i);
+  }
+  *nout = n;
+  lua_settop(L, top);
+  return 0;
+}
+
 /* ---- function-level access to the reference objects ------------------------------- */
 
 static MaraApplication *app(void) { return HydroModule::Mara; }
+
+/* GodunovOperator's FailureMask and the application's PrimitiveArray (the state the next
+ * Mara.diffuse reads), copied out: n entries / n doubles at most; returns the count. */
+long ref_failure_mask(int *out, long n)
+{
+  const std::valarray<int> &m = app()->FailureMask;
+  long k = 0;
+  for (; k < (long) m.size() && k < n; ++k) out[k] = m[k];
+  return k;
+}
+
+long ref_primitive_array(double *out, long n)
+{
+  const std::valarray<double> &P = app()->PrimitiveArray;
+  long k = 0;
+  for (; k < (long) P.size() && k < n; ++k) out[k] = P[k];
+  return k;
+}
 
 int ref_prim_to_cons(const double *P, double *U)
 {

@@ -12,6 +12,9 @@ Fixtures (all float64, AoS primitive layout with 3 guard zones where a grid is i
   flux.npz        FluxAndEigenvalues on random prims, dims 1..3
   riemann_*.npz   IntercellFlux of HLL / HLLC / HLLD on random face pairs
   recon.npz       PLM (theta=2) and WENO5-FV (JS96, B08, SZ10) on random stencils
+  c2p_paths.npz, riemann_hlld_paths.npz
+                  states chosen by the branch the reference takes on them (path_fixtures)
+  diffuse.npz     Mara.diffuse after a failed step / set_failmask, and Mara.measure.*
   divb.npz        measure.mean_max_divB / max_lorentz_factor on the step fixtures' states
 """
 from __future__ import annotations
@@ -187,6 +190,151 @@ def function_fixtures():
     np.savez_compressed(os.path.join(OUT, "recon.npz"), **out)
 
 
+def path_fixtures():
+    """States chosen by the path the reference's algorithm takes on them, so that every
+    branch is pinned one by one (the random fixtures above resolve almost all on the first):
+
+    c2p_paths.npz          conserved states whose gamma-law ladder (Mara/rmhd.cpp:103-176)
+                           resolves on rung 2 (Anton from the previous primitives), 3 (Noble
+                           from the estimate) or 4 (Noble from the previous primitives), or on
+                           none; `rung` is that class
+    riemann_hlld_paths.npz face pairs on which HLLD (Mara/riemann_hlld-rmhd.cpp:199-277)
+                           succeeds on its 2nd or 3rd pressure guess, or falls back to HLLC
+                           after all three fail or after its HLL-state c2p fails; `path` is
+                           1-3 (attempt), 4 (all failed) or 0 (HLL c2p failed)
+
+    The class comes from the C restatement (oracle/port, bit-exact with the reference on every
+    other fixture); the golden outputs come from the compiled reference."""
+    from oracle import PortOracle
+    rng = np.random.default_rng(77)
+    port = PortOracle(Scheme(n=(4, 4, 4)))
+    want = {2: 60, 3: 60, 4: 40, 0: 30}
+    picked = {k: [] for k in want}
+    while any(len(picked[k]) < want[k] for k in want):
+        P = random_prims(rng, 2000, wmax=float(rng.choice([10, 100, 1000])),
+                         sigma_max=float(rng.choice([10, 1e3, 1e5])), pmin=1e-8)
+        for p in P:
+            U, _ = port.prim_to_cons(p)
+            g = p * (1 + float(rng.choice([1e-9, 1e-6, 1e-3])) * rng.standard_normal(8))
+            r = [port.c2p_solve(U, s_, gg, g)[1] for s_, gg in ((0, 0), (0, 1), (1, 0), (1, 1))]
+            k = next((i + 1 for i, e in enumerate(r) if e == 0), 0)
+            if k in want and len(picked[k]) < want[k]:
+                picked[k].append((U, g, k))
+    rows = [x for k in (2, 3, 4, 0) for x in picked[k]]
+    U = np.array([x[0] for x in rows])
+    G = np.array([x[1] for x in rows])
+    rung = np.array([x[2] for x in rows])
+    ref = RefOracle(Scheme(n=(4, 4, 4)))
+    ladder = [ref.cons_to_prim(u, guess=g) for u, g in zip(U, G)]
+    solvers = {}
+    for solver in (0, 1):
+        for gm in (0, 1):
+            res = [ref.c2p_solve(u, solver, gm, g) for u, g in zip(U, G)]
+            solvers[f"P_{solver}{gm}"] = np.array([x[0] for x in res])
+            solvers[f"err_{solver}{gm}"] = np.array([x[1] for x in res])
+            solvers[f"it_{solver}{gm}"] = np.array([x[2] for x in res])
+    ref.close()
+    np.savez_compressed(os.path.join(OUT, "c2p_paths.npz"), U=U, guess=G, rung=rung,
+                        P_ladder=np.array([x[0] for x in ladder]),
+                        err_ladder=np.array([x[1] for x in ladder]), **solvers)
+    print("c2p_paths: rungs", {k: int((rung == k).sum()) for k in want})
+
+    port = PortOracle(Scheme(n=(4, 4, 4), riemann="hlld"))
+    want = {2: 50, 3: 50, 4: 50, 0: 40}
+    picked = {k: [] for k in want}
+    while any(len(picked[k]) < want[k] for k in want):
+        Pl = random_prims(rng, 500, wmax=float(rng.choice([2, 5, 20])),
+                          sigma_max=float(rng.choice([1, 10, 100])), pmin=1e-4)
+        Pr = Pl * (1 + float(rng.choice([0.05, 0.3, 1.0])) * rng.standard_normal(Pl.shape))
+        Pr[:, 0:2] = np.abs(Pr[:, 0:2])
+        vr = Pr[:, 2:5]
+        sp = np.linalg.norm(vr, axis=1)
+        Pr[:, 2:5] = np.where((sp > 0.99)[:, None], vr * (0.99 / sp)[:, None], vr)
+        for i in range(len(Pl)):
+            d = int(rng.integers(1, 4))
+            port.riemann(Pl[i], Pr[i], d)
+            k = port.stats.hlld_path
+            if k in want and len(picked[k]) < want[k]:
+                picked[k].append((Pl[i], Pr[i], d, k))
+    rows = [x for k in (2, 3, 4, 0) for x in picked[k]]
+    Pl = np.array([x[0] for x in rows])
+    Pr = np.array([x[1] for x in rows])
+    dims = np.array([x[2] for x in rows])
+    path = np.array([x[3] for x in rows])
+    ref = RefOracle(Scheme(n=(4, 4, 4), riemann="hlld"))
+    F = np.zeros((len(rows), 8))
+    err = np.zeros(len(rows), dtype=int)
+    mls = np.zeros(len(rows))
+    for i in range(len(rows)):
+        ref.lib.ref_reset_max_lambda()
+        F[i], err[i] = ref.riemann(Pl[i], Pr[i], int(dims[i]))
+        mls[i] = ref.max_lambda
+    ref.close()
+    np.savez_compressed(os.path.join(OUT, "riemann_hlld_paths.npz"), Pl=Pl, Pr=Pr, dim=dims, path=path,
+                        F=F, err=err, max_lambda=mls)
+    print("riemann_hlld_paths:", {k: int((path == k).sum()) for k in want})
+
+
+def diffuse_fixtures():
+    """diffuse.npz: Mara.diffuse (Mara/mara.cpp:343-366) and the eight other Mara.measure.*
+    (Mara/mara.cpp:1954-2230), from the compiled reference.
+
+    Cases (prefix c<k>_): 0 -- the 12^3 HLLC/RK3 turbulence box whose third step fails c2p
+    in one zone (its four copies): diffuse(P, 0.2) of the state before that step, with the
+    reference's own FailureMask and PrimitiveArray after the failed advance; 1 -- a 2D
+    Kelvin-Helmholtz box after one step with set_failmask(1) (diffusion on every face,
+    flux-CT in 2D), r = 0.3; 2 -- a 1D line after one step, set_failmask(1), r = 0.5.
+    Stored per case: scheme, P0 (the initial state), dts (the advances from it, after the
+    priming advance(P0, 0)), P (the diffuse's input), mask, PA (what the diffuse reads), Q (the
+    result), mask_out, and the measures of Q."""
+    out = {}
+    names = ["mean_cons", "mean_prim", "mean_energies", "mean_velocity", "mean_max_temperature",
+             "mean_max_magnetic_field", "mean_max_sonic_mach", "mean_min_alfvenic_mach"]
+    cases = [
+        (dict(n=(12, 12, 12), riemann="hllc", advance="rk3"), lambda: ics.turbulence_box((12, 12, 12), seed=1),
+         None, 0.2),
+        (dict(n=(24, 16), x0=(0.0, 0.0), x1=(1.0, 1.0), riemann="hlld", advance="rk2"),
+         lambda: ics.kh_box((24, 16), seed=31), 1, 0.3),
+        (dict(n=(40,), x0=(0.0,), x1=(1.0,), riemann="hlld", advance="rk3"), lambda: _line((40,), seed=32), 1, 0.5),
+    ]
+    for k, (kw, ic, failmask, r) in enumerate(cases):
+        ref = RefOracle(Scheme(**kw))
+        P = ic()
+        P0 = P.copy()
+        ref.advance(P, 0.0)
+        dts = []
+        while True:
+            dt = ref.get_timestep(0.3)
+            dts.append(dt)
+            Pb = P.copy()
+            e = ref.advance(P, dt)
+            if failmask is not None or e:
+                break
+            assert len(dts) < 10, "the failing step was not reached"
+        if failmask is not None:
+            ref.set_failmask(failmask)
+            Pb = P.copy()
+        mask, PA = ref.failure_mask(), ref.primitive_array()
+        Q = Pb.copy()
+        ref.diffuse(Q, r)
+        out[f"c{k}_scheme"] = np.array(repr(kw))
+        out[f"c{k}_failmask"] = np.array(-1 if failmask is None else failmask)
+        out[f"c{k}_r"] = np.array(r)
+        out[f"c{k}_dts"] = np.array(dts)
+        out[f"c{k}_P0"] = P0
+        out[f"c{k}_P"] = Pb
+        out[f"c{k}_mask"] = mask
+        out[f"c{k}_PA"] = PA.reshape(Pb.shape)
+        out[f"c{k}_Q"] = Q
+        out[f"c{k}_mask_out"] = ref.failure_mask()
+        for nm in names:
+            out[f"c{k}_{nm}"] = np.array(ref.measure(nm, Q))
+        print(f"diffuse case {k}: mask {int(mask.sum())}, changed zones "
+              f"{int((np.abs(Q - Pb).reshape(-1, 8).max(1) > 0).sum())}")
+        ref.close()
+    np.savez_compressed(os.path.join(OUT, "diffuse.npz"), **out)
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]          # fixture names to (re)generate; none: all of them
     for name, (kw, ic, steps, cfl) in STEP_CASES.items():
@@ -194,5 +342,9 @@ if __name__ == "__main__":
             step_fixture(name, kw, ic, steps, cfl)
     if not only or "functions" in only:
         function_fixtures()
+    if not only or "paths" in only:
+        path_fixtures()
+    if not only or "diffuse" in only:
+        diffuse_fixtures()
     total = sum(os.path.getsize(os.path.join(OUT, f)) for f in os.listdir(OUT) if f.endswith(".npz"))
     print(f"wrote {total / 1e6:.2f} MB of fixtures")

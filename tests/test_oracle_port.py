@@ -158,3 +158,57 @@ def test_whole_step_weno5_smoothness_indicators_against_the_compiled_reference(I
             assert np.array_equal(A, B)
     finally:
         ref.close()
+
+
+def test_c2p_paths_bitexact(golden):
+    """States that the reference's ladder resolves on rung 2, 3 or 4, or on none: the ladder
+    (previous primitives = the stored guess) and each solver from each starting point."""
+    g = golden("c2p_paths.npz")
+    port = PortOracle(Scheme(n=(4, 4, 4)))
+    assert set(np.unique(g["rung"])) == {0, 2, 3, 4}
+    for i, U in enumerate(g["U"]):
+        P, e = port.cons_to_prim(U, guess=g["guess"][i])
+        assert e == g["err_ladder"][i]
+        assert np.array_equal(P, g["P_ladder"][i])
+        for solver in (0, 1):
+            for guess in (0, 1):
+                P, e, it = port.c2p_solve(U, solver, guess, g["guess"][i])
+                assert e == g[f"err_{solver}{guess}"][i]
+                assert it == g[f"it_{solver}{guess}"][i]
+                if e == 0:
+                    assert np.array_equal(P, g[f"P_{solver}{guess}"][i])
+
+
+def test_hlld_paths_bitexact(golden):
+    """Faces on which HLLD succeeds on its 2nd or 3rd pressure guess, or falls back to HLLC
+    (all guesses failed, or its HLL-state c2p failed)."""
+    g = golden("riemann_hlld_paths.npz")
+    port = PortOracle(Scheme(n=(4, 4, 4), riemann="hlld"))
+    assert set(np.unique(g["path"])) == {0, 2, 3, 4}
+    for i in range(len(g["Pl"])):
+        port.stats.max_lambda = 0.0
+        F, e = port.riemann(g["Pl"][i], g["Pr"][i], int(g["dim"][i]))
+        assert port.stats.hlld_path == g["path"][i]
+        assert e == g["err"][i]
+        if e == 0:
+            assert np.array_equal(F, g["F"][i]), i
+        assert port.max_lambda == g["max_lambda"][i]
+
+
+MEASURE_NAMES = ["mean_cons", "mean_prim", "mean_energies", "mean_velocity", "mean_max_temperature",
+                 "mean_max_magnetic_field", "mean_max_sonic_mach", "mean_min_alfvenic_mach"]
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_diffuse_and_measures_bitexact(golden, k):
+    """Mara.diffuse with the reference's FailureMask and PrimitiveArray (after a failed step in
+    3D, after set_failmask(1) in 2D and 1D), then the eight Mara.measure.* of the result."""
+    g = golden("diffuse.npz")
+    kw = ast.literal_eval(str(g[f"c{k}_scheme"]))
+    port = PortOracle(Scheme(**kw))
+    Q = np.ascontiguousarray(g[f"c{k}_P"]).copy()
+    mask, e = port.diffuse(Q, float(g[f"c{k}_r"]), g[f"c{k}_mask"], g[f"c{k}_PA"])
+    assert np.array_equal(Q, g[f"c{k}_Q"])
+    assert np.array_equal(mask, g[f"c{k}_mask_out"])
+    for name in MEASURE_NAMES:
+        assert port.measure(name, Q) == list(g[f"c{k}_{name}"]), name

@@ -56,7 +56,15 @@ WORKLOADS = {
     # profiling size: the face array (166^3 x 8 x 4 B = 146 MB) still exceeds the 126 MB L2
     "turb160_weno5_hlld_rk3": ((160, 160, 160), "turbulence",
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
-    "stress512_plm_hlld_rk3": ((512, 512, 512), "stress", dict(extrap="plm", riemann="hlld", advance="rk3")),
+    # the high-magnetisation stress box (W log-uniform in [1, 10], sigma log-uniform in
+    # [0.1, 10], p = 0.01): the reference's algorithm fails its first step, so it runs with the
+    # reference's emergency reset (config_solver{ereset = true, preset = 0.01, dreset = 1})
+    "stress512_plm_hlld_rk3": ((512, 512, 512), "stress",
+                               dict(extrap="plm", riemann="hlld", advance="rk3", ereset=True, preset=0.01,
+                                    dreset=1.0)),
+    "stress128_plm_hlld_rk3": ((128, 128, 128), "stress",
+                               dict(extrap="plm", riemann="hlld", advance="rk3", ereset=True, preset=0.01,
+                                    dreset=1.0)),
 }
 DEFAULT_WORKLOAD = "turb512_plm_hlld_rk3"
 # ensembles: 256 independent 2D Kelvin-Helmholtz boxes, sides log-uniform in 64..512
@@ -216,14 +224,14 @@ def rel_l1(a, b, nd, ng=3):
     return out
 
 
-def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0, warmup=0):
+def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0, warmup=0, ic="turbulence"):
     """Time the reference's CPU advance (or the C restatement) on a bounded sample box, after
     `warmup` untimed advances."""
     from oracle import PortOracle, REF_SO, RefOracle, Scheme
     sch = Scheme(n=(n, n, n), **scheme_kw)
     kind = "reference" if (use_ref and os.path.exists(REF_SO)) else "port"
     o = RefOracle(sch) if kind == "reference" else PortOracle(sch)
-    P = make_ic("turbulence", (n, n, n), seed=seed)
+    P = make_ic(ic, (n, n, n), seed=seed)
     o.advance(P, 0.0)
     dt = o.get_timestep(CFL)
     for _ in range(warmup):
@@ -238,8 +246,8 @@ def cpu_sample(scheme_kw, steps=2, n=64, use_ref=True, seed=0, warmup=0):
 
 
 def _cpu_worker(args):
-    scheme_kw, steps, n, seed, warmup = args
-    return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed, warmup=warmup)
+    scheme_kw, steps, n, seed, warmup, ic = args
+    return cpu_sample(scheme_kw, steps=steps, n=n, seed=seed, warmup=warmup, ic=ic)
 
 
 def cpu_sample_kh(scheme_kw, steps=2, n=256, seed=0, warmup=0):
@@ -574,10 +582,11 @@ def run_reference_arm(args, wl_name, rank, world):
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+    ic = "turbulence"
     if wl_name in DRIVEN_WORKLOADS:
         n_wl, scheme_kw = DRIVEN_WORKLOADS[wl_name]["n"], DRIVEN_WORKLOADS[wl_name]["scheme"]
     else:
-        n_wl, _, scheme_kw = WORKLOADS[wl_name]
+        n_wl, ic, scheme_kw = WORKLOADS[wl_name]
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     n = 64 if n_wl[0] >= 64 else n_wl[0]
@@ -585,7 +594,7 @@ def run_reference_arm(args, wl_name, rank, world):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s, args.warmup) for s in range(cores)])
+        res = pool.map(_cpu_worker, [(scheme_kw, steps, n, s, args.warmup, ic) for s in range(cores)])
     wall = time.perf_counter() - t0
     kind = res[0][0]
     measured = float(sum(r[1] for r in res))
@@ -600,7 +609,7 @@ def run_reference_arm(args, wl_name, rank, world):
                    "scheme": scheme_kw, "cfl": CFL},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "measured_value": measured, "ghost_correction": corr,
-                         "sample": f"{cores} concurrent replicas x {steps} steps of a {n}^3 turbulence "
+                         "sample": f"{cores} concurrent replicas x {steps} steps of a {n}^3 {ic} "
                                    f"box ({scheme_kw}), interior zone-updates/s summed; wall {wall:.1f} s; "
                                    f"value = measured x {corr:.3f}, the ratio of guarded to interior zones "
                                    f"of the sample to that of the {n_wl[0]}^3 workload (the reference "
@@ -739,6 +748,10 @@ def main():
         return st["c2p_iters"] / max(st["c2p_calls"], 1)
     out["runs"] = {k: {"value": r["value"], "ms_per_step": r["ms_per_step"],
                        "c2p_iters_per_call": c2p_it(k), "errors": r["errors"],
+                       # zone c2p calls that failed every rung of the ladder (with the
+                       # emergency reset these are the resets), per call, last advance
+                       "c2p_failed_per_call": r["stats"]["c2p_failed"] / max(r["stats"]["c2p_calls"], 1),
+                       "c2p_attempt": r["stats"]["c2p_attempt"],
                        "failed_steps": r["failed_advances"],
                        "kernel_ms_per_step": {c: r["prof"][c]["ms"] / args.steps for c in r["prof"]}}
                    for k, r in results.items()}
@@ -829,8 +842,9 @@ def main():
             gbs = per_unit[k] * pk["units"] / (pk["ms"] * 1e-3) / 1e9
             out["kernels"][k] = {"ms_per_launch": pk["ms"] / pk["launches"], "bytes_per_unit": per_unit[k],
                                  "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / hbm}
-    out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "c2p_attempt", "face_c2p_calls",
-                                                      "face_c2p_iters", "hlld_ok", "hlld_hllc", "pcm_retry")}
+    out["c2p_stats"] = {k: head["stats"][k] for k in ("c2p_calls", "c2p_iters", "c2p_attempt", "c2p_failed",
+                                                      "face_c2p_calls", "face_c2p_iters", "hlld_ok", "hlld_hllc",
+                                                      "pcm_retry")}
 
     # end to end through Mara.advance(buf, dt) semantics with pinned host buffers
     if not args.no_e2e:
@@ -861,11 +875,11 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ns_cpu = 48
-        kind, v, sec = cpu_sample(scheme_kw, steps=2, n=ns_cpu)
+        kind, v, sec = cpu_sample(scheme_kw, steps=2, n=ns_cpu, ic=ic_kind)
         corr = ghost_factor(ns_cpu, n)
         out["cpu_baseline"] = {"value": v * corr, "unit": UNIT, "cores": 1, "kind": kind,
                                "measured_value": v, "ghost_correction": corr,
-                               "sample": f"{ns_cpu}^3 turbulence box, same scheme, 2 steps after priming "
+                               "sample": f"{ns_cpu}^3 {ic_kind} box, same scheme, 2 steps after priming "
                                          f"({sec:.1f} s), interior zone-updates/s on 1 core; value = measured x "
                                          f"{corr:.3f}, the ratio of guarded to interior zones of the sample to that "
                                          f"of the {n[0]}^3 workload (the reference advances every guard zone)"}

@@ -37,7 +37,8 @@ class MgpuStats(ctypes.Structure):
                 ("c2p_iters", ctypes.c_ulonglong), ("c2p_attempt", ctypes.c_ulonglong * 6),
                 ("face_c2p_calls", ctypes.c_ulonglong), ("face_c2p_iters", ctypes.c_ulonglong),
                 ("hlld_ok", ctypes.c_ulonglong), ("hlld_hllc", ctypes.c_ulonglong),
-                ("pcm_retry", ctypes.c_ulonglong), ("advances", ctypes.c_ulonglong),
+                ("pcm_retry", ctypes.c_ulonglong), ("c2p_failed", ctypes.c_ulonglong),
+                ("advances", ctypes.c_ulonglong),
                 ("failed_advances", ctypes.c_ulonglong), ("failed_zones", ctypes.c_ulonglong)]
 
     def as_dict(self) -> dict:

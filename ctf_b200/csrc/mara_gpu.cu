@@ -635,6 +635,7 @@ int mgpu_get_stats(mgpu_solver *h, mgpu_stats *s)
   s->hlld_ok = t.hlld_ok;
   s->hlld_hllc = t.hlld_hllc;
   s->pcm_retry = t.pcm_retry;
+  s->c2p_failed = t.c2p_failed;
   s->advances = c.n_advances;
   s->failed_advances = c.n_failed;
   s->failed_zones = c.n_failed_zones;

@@ -43,7 +43,8 @@ struct StatSlot {
   unsigned long long c2p_calls, c2p_iters, c2p_attempt[6];
   unsigned long long face_c2p_calls, face_c2p_iters;
   unsigned long long hlld_ok, hlld_hllc, pcm_retry;
-  unsigned long long pad[3];   // 128 bytes
+  unsigned long long c2p_failed;   // zone c2p calls that failed every rung (reset or not)
+  unsigned long long pad[2];       // 128 bytes
 };
 
 // What a c2p launch reads, where it writes and which counter its failures go to.
@@ -100,6 +101,7 @@ inline StatSlot stat_sum(const Ctl &c)
     t.hlld_ok += s.hlld_ok;
     t.hlld_hllc += s.hlld_hllc;
     t.pcm_retry += s.pcm_retry;
+    t.c2p_failed += s.c2p_failed;
   }
   return t;
 }

@@ -83,6 +83,8 @@ typedef struct {
   unsigned long long face_c2p_calls, face_c2p_iters; /* HLL-state c2p inside HLLD */
   unsigned long long hlld_ok, hlld_hllc, pcm_retry;  /* HLLD successes / HLLC fallbacks /
                                                         PCM retries of a face */
+  unsigned long long c2p_failed;                     /* zone c2p calls that failed every rung of the
+                                                        ladder (emergency resets included) */
   unsigned long long advances, failed_advances,      /* since mgpu_set_domain: advances run, those */
                      failed_zones;                   /* not committed, and the failed zones
                                                         they reported (sum of their `errors`) */

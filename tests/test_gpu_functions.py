@@ -5,9 +5,10 @@ time, through the C ABI's mgpu_probe_* entry points.
 Bit for bit where the arithmetic is the reference's operation sequence (P->U, the c2p
 solvers and their iteration counts, PLM/WENO5 reconstruction, the physical flux).  Where the
 fast wave speeds enter (the quartic's pow/acos/cos/sin from CUDA's libm, which differ from
-glibc by a few ulp) the eigenvalues are held to LIBM_REL.  A Riemann flux amplifies its wave speeds' rounding by up to |F| / (lambda+ - lambda-): the
-fluxes are held to RIEMANN_REL (the whole-step bound) face by face, and most faces (at least
-BITLIKE_SHARE of them) to 1e-14.
+glibc by a few ulp) the eigenvalues of the flux fixture are held to LIBM_REL.  A Riemann flux amplifies its wave speeds' rounding by up to |F| / (lambda+ - lambda-): the
+fluxes and the faces' MaxLambda (where a near-degenerate pair of roots of the quartic can
+amplify the libm difference too) are held to RIEMANN_REL (the whole-step bound) face by face,
+and most faces (at least BITLIKE_SHARE of them) to 1e-14.
 The path fixtures hold states on which the reference takes its rarer branches -- the c2p
 ladder's rungs 2-4 and HLLD's second and third pressure guesses and its HLLC fallback -- so
 each branch is pinned on the device, error codes and iteration counts included.
@@ -170,7 +171,8 @@ def test_riemann_random_faces(golden, solver, name):
         rel = face_rel(F[ok], g["F"][d][ok])
         assert rel.max() <= RIEMANN_REL, rel.max()
         assert (rel <= 1e-14).mean() >= BITLIKE_SHARE, (rel <= 1e-14).mean()
-        assert np.abs(ml - g["max_lambda"][d]).max() <= LIBM_REL * np.abs(g["max_lambda"][d]).max()
+        mrel = np.abs(ml - g["max_lambda"][d]) / np.abs(g["max_lambda"][d])
+        assert mrel.max() <= RIEMANN_REL and (mrel <= 1e-14).mean() >= BITLIKE_SHARE, mrel.max()
 
 
 def test_hlld_second_third_guess_and_hllc_fallback(golden):
@@ -185,7 +187,8 @@ def test_hlld_second_third_guess_and_hllc_fallback(golden):
     rel = face_rel(F[ok], g["F"][ok])
     assert rel.max() <= RIEMANN_REL, rel.max()
     assert (rel <= 1e-14).mean() >= BITLIKE_SHARE, (rel <= 1e-14).mean()
-    assert (np.abs(ml - g["max_lambda"]) <= LIBM_REL * np.abs(g["max_lambda"])).all()
+    mrel = np.abs(ml - g["max_lambda"]) / np.abs(g["max_lambda"])
+    assert mrel.max() <= RIEMANN_REL and (mrel <= 1e-14).mean() >= BITLIKE_SHARE, mrel.max()
 
 
 # ---- reconstruction --------------------------------------------------------------------

@@ -160,9 +160,9 @@ def test_scheme_change_in_place_keeps_state_and_max_lambda():
     from oracle import RefOracle, Scheme as OScheme
     n = (8, 8, 8)
     P0 = ics.turbulence_box(n, seed=44, vrms=0.3)
-    ref = RefOracle(OScheme(n=n, riemann="hllc", advance="rk2"))
+    ref = RefOracle(OScheme(n=n, riemann="hll", advance="rk2"))
     try:
-        s = Solver(Scheme(riemann="hllc", advance="rk2"), n)
+        s = Solver(Scheme(riemann="hll", advance="rk2"), n)
         A = P0.copy()
         s.upload(P0.copy())
         assert ref.advance(A, 0.0) == 0 and s.advance(0.0) == 0

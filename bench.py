@@ -53,9 +53,11 @@ WORKLOADS = {
                              dict(extrap="plm", riemann="hlld", advance="rk3")),
     "turb128_weno5_hlld_rk3": ((128, 128, 128), "turbulence",
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
-    # profiling size: the face array (166^3 x 8 x 4 B = 146 MB) still exceeds the 126 MB L2
+    # profiling sizes: the face array (166^3 x 8 x 4 B = 146 MB) still exceeds the 126 MB L2
     "turb160_weno5_hlld_rk3": ((160, 160, 160), "turbulence",
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
+    "turb160_plm_hlld_rk3": ((160, 160, 160), "turbulence",
+                             dict(extrap="plm", riemann="hlld", advance="rk3")),
     # the high-magnetisation stress box (W log-uniform in [1, 10], sigma log-uniform in
     # [0.1, 10], p = 0.01): the reference's algorithm fails its first step, so it runs with the
     # reference's emergency reset (config_solver{ereset = true, preset = 0.01, dreset = 1})

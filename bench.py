@@ -557,6 +557,92 @@ def run_driven_bench(args, rank, world, local):
         print(json.dumps(out), flush=True)
 
 
+def tiled_block(tile: np.ndarray, off, n, ng=3) -> np.ndarray:
+    """The guarded block [off - ng, off + n + ng) of the periodic box made by repeating the
+    interior of `tile` (a guarded turbulence box) along every axis: a large periodic state
+    whose blocks each rank builds on its own, without the global array."""
+    t = tile[ng:-ng, ng:-ng, ng:-ng]
+    idx = [np.arange(o - ng, o + m + ng) % t.shape[d] for d, (o, m) in enumerate(zip(off, n))]
+    return np.ascontiguousarray(t[np.ix_(*idx)])
+
+
+def run_decomposed_bench(args, rank, world, local):
+    """--decompose: one box of the workload split over the ranks (DecomposedSolver, standard
+    layout, FP32 bulk + learned c2p as the headline run), the guard exchange of every RK stage
+    over NCCL overlapped with the cores' c2p: strong scaling.  The state is a 128^3 turbulence
+    box repeated periodically to the workload's size (each rank builds only its block)."""
+    import torch
+    from ctf_b200 import ics
+    from ctf_b200.decomp import DecomposedSolver, Layout, TorchTransport, rank_dims
+    from ctf_b200.mara import Scheme
+    dist = None
+    torch.cuda.set_device(local if world > 1 else 0)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    n, _, scheme_kw = WORKLOADS[args.workload]
+    net_path = os.path.join(ROOT, "ctf_b200", "data", "c2p_net.npz")
+    learned = os.path.exists(net_path) and not args.no_learned
+    scheme = Scheme(precision="fp32", learned_c2p=learned, **scheme_kw)
+    dims = rank_dims(world, 3, n)
+    L = Layout(N=n, dims=dims, x0=(0.0,) * 3, x1=(1.0,) * 3)
+    D = DecomposedSolver(scheme, L, ranks=[rank], transport=TorchTransport(dist) if dist else None)
+    if learned:
+        from ctf_b200.train_c2p import load as load_net
+        for b in D.blocks:
+            b.solver.set_c2p_network(load_net(net_path))
+    tile = ics.turbulence_box((128, 128, 128), seed=0)
+    for b in D.blocks:
+        b.solver.upload(tiled_block(tile, b.off, b.n))
+    D.advance(dt=0.0)
+    assert D.errors() == 0, "priming advance failed"
+    dt = D.get_timestep(CFL)
+    for _ in range(args.warmup):
+        D.advance(dt=dt)
+    D.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(D.stream)
+        for _ in range(args.steps):
+            D.advance(dt=dt)
+        end.record(D.stream)
+        end.synchronize()
+    ms = start.elapsed_time(end)
+    errs = D.errors()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    zones = int(np.prod(n))
+    nst = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}[scheme_kw["advance"]]
+    # per advance: begin + per stage (shell c2p, core c2p, 3 sweeps, update) + closing c2p +
+    # commit, plus 4 slab pack/unpack kernels per split dimension and stage
+    per_adv = 2 + nst * (2 + 3 + 1) + 1 + nst * 4 * len(L.split())
+    out = {"metric": METRIC, "value": zones * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": args.workload, "n": list(n), "scheme": scheme_kw, "cfl": CFL, "dt": dt,
+                      "layout": "standard", "decomposition": list(dims),
+                      "precision": "fp32 bulk; fp64 c2p polish, magnetic field, CT and dt"
+                                   + ("; learned c2p guess" if learned else ""),
+                      "ic": "128^3 turbulence box repeated periodically",
+                      "exchange": "NCCL point-to-point per RK stage, overlapped with the cores' c2p",
+                      "l2": "every state array > 126 MB L2 (no flush needed)",
+                      "parallelism": f"{world} ranks, one box"},
+           "gpu_launches": per_adv * args.steps, "clocks": clk.summary(), "errors": errs,
+           "e2e": None, "e2e_note": "the decomposed mode keeps the state on the devices (no host copies)"}
+    D.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def run_reference_arm(args, wl_name, rank, world):
     """--impl reference: the reference's own CPU advance on every host core (independent
     replicas of a 64^3 sample box of the workload's scheme, or 256^2 KH boxes for an
@@ -635,6 +721,9 @@ def main():
     ap.add_argument("--skip-fp64-fmad", action="store_true",
                     help="leave out the comparator run of the FP64 kernels compiled with FMA contraction")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--decompose", action="store_true",
+                    help="split one box of the workload over the ranks (strong scaling) instead of "
+                         "advancing one box per rank (weak scaling)")
     ap.add_argument("--layout", default="lean", choices=["standard", "lean"],
                     help="device layout of the FP32 runs of the turbulence workloads (lean: 3D, 144 B per "
                          "zone in FP32; the FP64 run always uses the standard layout)")
@@ -652,6 +741,9 @@ def main():
         return
     if args.workload in DRIVEN_WORKLOADS:
         run_driven_bench(args, rank, world, local)
+        return
+    if args.decompose:
+        run_decomposed_bench(args, rank, world, local)
         return
 
     import torch

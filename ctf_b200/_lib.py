@@ -160,6 +160,8 @@ SIGNATURES = {
     "mgpu_diffuse_host": (ctypes.c_int, [_vp, _dp, ctypes.c_double, _ip]),
     "mgpu_set_failmask": (ctypes.c_int, [_vp, ctypes.c_int]),
     "mgpu_reconfigure": (ctypes.c_int, [_vp, ctypes.POINTER(MgpuConfig)]),
+    "mgpu_halo_pack_on": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "mgpu_halo_unpack_on": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
 }
 
 

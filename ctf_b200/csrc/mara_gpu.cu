@@ -978,9 +978,10 @@ int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double
   int rc = ensure_ready(h);
   if (rc) return rc;
   const int ns = num_stages(h->cfg.rk);
-  if (phase < 0 || phase > 3 || stage < 0 || stage > ns || (phase == 2 && stage >= ns) ||
+  if (phase < 0 || phase > 5 || stage < 0 || stage > ns || ((phase == 2 || phase >= 4) && stage >= ns) ||
       (dt_mode != 0 && dt_mode != 1))
     return fail(h, MGPU_ERR_ARG, "bad advance phase arguments");
+  if (phase >= 4 && lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   AdvanceArgs A;
   A.g = h->g;
   A.pp = phys(h);
@@ -1061,7 +1062,8 @@ int mgpu_halo_bytes(mgpu_solver *h, int which, int dim, long long *bytes)
   return MGPU_OK;
 }
 
-static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pack)
+static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pack, cudaStream_t stream = nullptr,
+                bool use_stream = false)
 {
   int rc = ensure_ready(h);
   if (rc) return rc;
@@ -1069,6 +1071,7 @@ static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pac
     return fail(h, MGPU_ERR_ARG, "bad halo arguments");
   if (lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   TransferArgs t = transfer_args(h);
+  if (use_stream) t.stream = stream;
   if (which == 1) {
     rc = read_ctl(h);
     if (rc) return rc;
@@ -1076,6 +1079,16 @@ static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pac
   }
   CK(fp32(h) ? halo_fp32(t, which, dim, side, buf, pack) : halo_fp64(t, which, dim, side, buf, pack));
   return MGPU_OK;
+}
+
+int mgpu_halo_pack_on(mgpu_solver *h, int which, int dim, int side, void *dev_buf, void *stream)
+{
+  return halo(h, which, dim, side, dev_buf, 1, (cudaStream_t) stream, true);
+}
+
+int mgpu_halo_unpack_on(mgpu_solver *h, int which, int dim, int side, const void *dev_buf, void *stream)
+{
+  return halo(h, which, dim, side, const_cast<void *>(dev_buf), 0, (cudaStream_t) stream, true);
 }
 
 int mgpu_halo_pack(mgpu_solver *h, int which, int dim, int side, void *dev_buf)

@@ -65,7 +65,9 @@ inline void launch_flux(const Grid &g, int d, int rs, unsigned grid, unsigned bl
 // buffer), then PH_COMMIT.  A decomposed domain exchanges the guard layers of the stage
 // primitives between PH_C2P and PH_FLUX_UPDATE, and sums the error counters over ranks
 // before PH_COMMIT.
-enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3 };
+// PH_C2P_SHELL and PH_C2P_CORE together are PH_C2P of a stage (s < number of stages), split
+// so that a decomposed domain can exchange the shell's slabs while the core converts.
+enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3, PH_C2P_SHELL = 4, PH_C2P_CORE = 5 };
 
 // The phases of an advance in the lean layout (rmhd_lean.cuh): no P->U (the committed state
 // is conserved), no c2p at the first stage, sweeps that accumulate into U[!cur], CT from the
@@ -148,6 +150,18 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     ProfScope ps(pr, st, KC_P2C, g.ninterior);
     k_prim_to_cons<T><<<zgrid, zb, 0, st>>>(g, cstate(b.Pc_bulk[0], b.Pc_B[0]), cstate(b.Pc_bulk[1], b.Pc_B[1]),
                                             U0, A.pp.gamma, A.ctl);
+  } else if (phase == PH_C2P_SHELL || phase == PH_C2P_CORE) {
+    const int final = A.godunov ? 2 : 0;
+    const StateCPtr<T> Uin = s == 0 ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B};
+    const bool learned = A.pp.learned && (A.pp.mlp_tc || A.pp.mlp);
+    if (learned) {   // the learned guess converts the whole interior in one pass: no split
+      if (phase == PH_C2P_SHELL) return launch_phase<T>(A, PH_C2P, s);
+      return cudaGetLastError();
+    }
+    ProfScope ps(pr, st, KC_C2P, g.ninterior);
+    k_cons_to_prim_region<T><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
+        g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, s == 0, final, A.ereset, A.preset, A.dreset,
+        phase == PH_C2P_SHELL ? 1 : 2);
   } else if (phase == PH_C2P) {
     // stage s < ns reads the stage input (U0 first, U1 after) into PA; s == ns is the
     // closing c2p of U0 into the uncommitted primitive buffer

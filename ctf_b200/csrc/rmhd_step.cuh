@@ -280,6 +280,41 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, Sta
                      final, ereset, preset, dreset, t);
 }
 
+// The boundary shell of a decomposed block: interior zones within Ng of a face whose guards a
+// halo exchange fills (region 1), and the rest (region 2, the core).  The exchange reads only
+// shell zones (and their periodic images along the unsplit dimensions), so the core's c2p can
+// run while the slabs travel.
+__device__ __forceinline__ bool in_shell(const Grid &g, int i, int j, int k)
+{
+  const int m[3] = {i, j, k};
+  for (int d = 0; d < 3; ++d) {
+    if (!g.ext[d]) continue;
+    const int r = m[d] - g.ng;
+    if (r < g.ng || r >= g.n[d] - g.ng) return true;
+  }
+  return false;
+}
+
+// The stage c2p of one region of the interior (1 shell, 2 core); zones of the other region
+// exit at once.
+template <class T>
+__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_region(Grid g, StateCPtr<T> U, T *PA,
+                                                                            StatePtr<T> Pn0, StatePtr<T> Pn1,
+                                                                            PhysParams pp, Ctl *ctl, int stage,
+                                                                            int zero_guess, int final, int ereset,
+                                                                            double preset, double dreset, int region)
+{
+  if (c2p_skip(ctl, stage, final)) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
+  int i, j, k;
+  interior_coords(g, t, i, j, k);
+  if (in_shell(g, i, j, k) != (region == 1)) return;
+  const int target = ctl->cur ^ 1;
+  c2p_zone<T, 2>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess, final,
+                 ereset, preset, dreset, t);
+}
+
 // ---- flux sweep (MethodOfLinesSplit::intercell_flux_sweep, Mara/plm-split.cpp:43-73) ---------
 // One thread per face.  The face set is the reference's: every zone index f with
 // 2*S <= f < nz - 3*S in the flattened guarded array (S the zone stride of `dim`), the face

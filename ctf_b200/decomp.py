@@ -10,7 +10,10 @@ the minimum dt over ranks (Mara/mara_mpi.c:96-130).
 Here a rank is one `mara.Solver` of its block.  `DecomposedSolver` drives its advance phase
 by phase (`mgpu_advance_phase`), exchanging the stage primitives' guard slabs between the
 c2p and the flux sweeps of every RK stage and reducing the error counters and MaxLambda
-before the commit; all of it stays on the device stream (no host synchronisation per step).
+before the commit; all of it stays on the device streams (no host synchronisation per step).
+The exchange overlaps the stage c2p: the boundary shell (zones within Ng of a split face,
+all the slabs read) converts first, the slabs travel on a side stream while the core
+converts, and the sweeps wait for both.
 Two transports move the slabs:
 
 * `TorchTransport` -- torch.distributed point-to-point (NCCL between GPUs; gloo on CPU
@@ -113,6 +116,17 @@ def unpack_slab(A: np.ndarray, buf: np.ndarray, dim: int, side: int, n: int, ng:
     shp = np.moveaxis(view, dim, 0).shape            # (ng, crossA, crossB, q)
     s = buf.reshape((A.shape[3], shp[0], shp[1], shp[2]))
     A[slab_index(A.shape[:3], dim, first, ng)] = np.moveaxis(np.moveaxis(s, 0, 3), 0, dim)
+
+
+def shell_mask(n, split, ng: int = NG) -> np.ndarray:
+    """Interior zones of a block (n per dimension, 3 entries) within ng of a face of a split
+    dimension: the zones the overlapped schedule converts before the exchange (the device's
+    in_shell)."""
+    idx = np.meshgrid(*[np.arange(m) for m in n], indexing="ij")
+    mask = np.zeros(tuple(n), dtype=bool)
+    for d in split:
+        mask |= (idx[d] < ng) | (idx[d] >= n[d] - ng)
+    return mask
 
 
 def periodic_fill(A: np.ndarray, dim: int, n: int, ng: int = NG):
@@ -223,6 +237,39 @@ def exchange_numpy(A: np.ndarray, layout: Layout, rank: int, transport) -> None:
         unpack_slab(A, recv_hi.numpy(), d, 1, n[d])
 
 
+def overlapped_exchange_numpy(truth: np.ndarray, layout: Layout, rank: int, transport) -> np.ndarray:
+    """The overlapped schedule on one rank's host block, as the device runs it: the block
+    starts unknown (NaN), the boundary shell's zones are converted (copied from `truth`, the
+    block's interior) with their images along the unsplit dimensions, the split dimensions'
+    slabs are exchanged, then the core's zones are converted with their images.  Returns the
+    block; it equals the whole-box periodic fill only if the exchange reads nothing but shell
+    zones."""
+    _, _, n, _, _ = layout.local(rank)
+    nd = layout.nd
+    n3 = tuple(n) + (1,) * (3 - nd)
+    A = np.full_like(truth, np.nan)
+    inner = tuple(slice(NG, NG + n3[d]) if d < nd else slice(None) for d in range(3))
+    shell = shell_mask(n3, layout.split())
+    for region in (shell, ~shell):
+        view = A[inner]
+        view[region] = truth[inner][region]
+        A[inner] = view
+        for d in range(nd):
+            if layout.dims[d] == 1:
+                periodic_fill(A, d, n[d])
+        if region is shell:
+            for d in layout.split():
+                low, high = neighbours(layout, rank, d)
+                import torch
+                send_lo = torch.from_numpy(pack_slab(A, d, 0, n[d]))
+                send_hi = torch.from_numpy(pack_slab(A, d, 1, n[d]))
+                recv_lo, recv_hi = torch.empty_like(send_hi), torch.empty_like(send_lo)
+                transport.exchange(send_lo, send_hi, recv_lo, recv_hi, low, high)
+                unpack_slab(A, recv_lo.numpy(), d, 0, n[d])
+                unpack_slab(A, recv_hi.numpy(), d, 1, n[d])
+    return A
+
+
 class _Block:
     """One rank's solver plus its slab buffers."""
 
@@ -254,16 +301,26 @@ class _Block:
     def phase(self, phase, stage=0, dt_mode=0, dt=0.0, cfl=0.0):
         self.solver._check(self.lib.mgpu_advance_phase(self.h, phase, stage, dt_mode, float(dt), float(cfl)))
 
-    def pack(self, which, d):
+    def pack(self, which, d, stream=None):
+        """The send slabs of dimension d, on the solver's stream or on `stream`."""
         b = self.bufs[(d, which)]
         for side in (0, 1):
-            self.solver._check(self.lib.mgpu_halo_pack(self.h, which, d, side, ctypes.c_void_p(b["send"][side].data_ptr())))
+            buf = ctypes.c_void_p(b["send"][side].data_ptr())
+            if stream is None:
+                self.solver._check(self.lib.mgpu_halo_pack(self.h, which, d, side, buf))
+            else:
+                self.solver._check(self.lib.mgpu_halo_pack_on(self.h, which, d, side, buf,
+                                                              ctypes.c_void_p(stream.cuda_stream)))
 
-    def unpack(self, which, d):
+    def unpack(self, which, d, stream=None):
         b = self.bufs[(d, which)]
         for side in (0, 1):
-            self.solver._check(self.lib.mgpu_halo_unpack(self.h, which, d, side,
-                                                         ctypes.c_void_p(b["recv"][side].data_ptr())))
+            buf = ctypes.c_void_p(b["recv"][side].data_ptr())
+            if stream is None:
+                self.solver._check(self.lib.mgpu_halo_unpack(self.h, which, d, side, buf))
+            else:
+                self.solver._check(self.lib.mgpu_halo_unpack_on(self.h, which, d, side, buf,
+                                                                ctypes.c_void_p(stream.cuda_stream)))
 
 
 class DecomposedSolver:
@@ -273,23 +330,29 @@ class DecomposedSolver:
     None every rank of the layout lives in this process on the current device (one shared
     stream, slabs copied directly)."""
 
-    def __init__(self, scheme, layout: Layout, ranks, transport=None, stream=None):
+    def __init__(self, scheme, layout: Layout, ranks, transport=None, stream=None, overlap=True):
         import torch
         layout.check()
         self.layout = layout
         self.scheme = scheme
         self.transport = transport
         self.stream = stream or torch.cuda.Stream()
+        # overlap: each stage converts the blocks' boundary shells first (phase 4), exchanges
+        # their slabs on a side stream while the cores convert (phase 5), and starts the sweeps
+        # once both are done; otherwise c2p, exchange and sweeps run one after the other
+        self.overlap = overlap
+        self.side = torch.cuda.Stream() if overlap else None
         self.blocks = [_Block(scheme, layout, r, self.stream.cuda_stream) for r in ranks]
         self.by_rank = {b.rank: b for b in self.blocks}
         self.ns = {"single": 1, "rk2": 2, "rk3": 3, "rk4": 4}[scheme.advance]
 
-    # -- guard exchange of every split dimension, in order x, y, z --
-    def exchange(self, which):
+    # -- guard exchange of every split dimension, in order x, y, z (on `stream`, or on the
+    # solvers' stream) --
+    def exchange(self, which, stream=None):
         L = self.layout
         for d in L.split():
             for b in self.blocks:
-                b.pack(which, d)
+                b.pack(which, d, stream)
             for b in self.blocks:
                 low, high = neighbours(L, b.rank, d)
                 buf = b.bufs[(d, which)]
@@ -300,7 +363,7 @@ class DecomposedSolver:
                 else:
                     self.transport.exchange(buf["send"][0], buf["send"][1], buf["recv"][0], buf["recv"][1], low, high)
             for b in self.blocks:
-                b.unpack(which, d)
+                b.unpack(which, d, stream)
 
     def _reduce(self):
         import torch
@@ -325,9 +388,19 @@ class DecomposedSolver:
             for b in self.blocks:
                 b.phase(0, 0, dt_mode, dt or 0.0, cfl or 0.0)
             for s in range(self.ns):
-                for b in self.blocks:
-                    b.phase(1, s)
-                self.exchange(0)
+                if self.overlap:
+                    for b in self.blocks:
+                        b.phase(4, s)                      # the shells the slabs read
+                    self.side.wait_stream(self.stream)
+                    with torch.cuda.stream(self.side):
+                        self.exchange(0, self.side)         # slabs travel ...
+                    for b in self.blocks:
+                        b.phase(5, s)                      # ... while the cores convert
+                    self.stream.wait_stream(self.side)
+                else:
+                    for b in self.blocks:
+                        b.phase(1, s)
+                    self.exchange(0)
                 for b in self.blocks:
                     b.phase(2, s)
             for b in self.blocks:

@@ -257,7 +257,8 @@ int mgpu_ou_field_advance(void *field, long long bytes, int nd, double dt);
  * and takes multiplicity tables: mult lists, for each such dimension in order and each
  * local interior index along it, how many guarded arrays over all ranks hold that zone (the
  * reference counts a failed zone once per array holding it, Mara/hydro.cpp:133-149,201).
- * The host then drives each advance phase by phase and fills the guards between them:
+ * The host then drives each advance phase by phase and fills the guards between them
+ * (phases 0 begin, 1 c2p, 2 flux+update, 3 commit; 4 and 5 below):
  *   mgpu_advance_phase(0 begin) ; per stage s: phase(1 c2p, s), exchange the stage
  *   primitives (which 0) for every split dimension in order x, y, z with
  *   mgpu_halo_pack / mgpu_halo_unpack, phase(2 flux+update, s) ; phase(1 c2p, stages) ;
@@ -274,6 +275,15 @@ int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult);  
 int mgpu_halo_bytes(mgpu_solver *h, int which, int dim, long long *bytes);
 int mgpu_halo_pack(mgpu_solver *h, int which, int dim, int side, void *dev_buf);
 int mgpu_halo_unpack(mgpu_solver *h, int which, int dim, int side, const void *dev_buf);
+/* Overlapped exchange (no counterpart in the reference, whose Synchronize blocks): phase 4
+ * converts the stage's boundary shell -- interior zones within Ng of a split face, all the
+ * slabs read -- and phase 5 the core; together they are phase 1 of that stage (s < stages;
+ * with a learned c2p network phase 4 converts everything and phase 5 nothing).  Between
+ * them the caller can pack, exchange and unpack on another stream (the _on variants, stream
+ * = cudaStream_t; order it after phase 4 and phase 2 after the unpacks with events) while
+ * phase 5 runs on the handle's stream: the core's c2p writes no zone a slab reads or fills. */
+int mgpu_halo_pack_on(mgpu_solver *h, int which, int dim, int side, void *dev_buf, void *stream);
+int mgpu_halo_unpack_on(mgpu_solver *h, int which, int dim, int side, const void *dev_buf, void *stream);
 
 /* ---- function-level probes (test infrastructure of the parity suite; no counterpart in
  * the reference's Lua API).  Each applies one FP64 device function of the advance to n

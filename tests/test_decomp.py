@@ -1,6 +1,7 @@
 """Domain decomposition host logic on the CPU: block geometry, the multiplicity tables of
-the error counts, the slab layout, and the guard exchange schedule across world_size-2 and
--4 gloo process groups (CPU tensors), against the periodic guard fill of the whole box."""
+the error counts, the slab layout, and the guard exchange schedule -- serial, and overlapped
+with the core's c2p (the slabs must read only boundary-shell zones) -- across world_size-2
+and -4 gloo process groups (CPU tensors), against the periodic guard fill of the whole box."""
 import os
 
 import numpy as np
@@ -91,6 +92,8 @@ def _worker(rank, world, port, N, dims, q):
             idx[d] = list(range(NG)) + list(range(n[d] + NG, n[d] + 2 * NG))
             A[tuple(idx)] = np.nan
         decomp.exchange_numpy(A, L, rank, decomp.TorchTransport(dist))
+        # the overlapped schedule: shells converted, slabs exchanged, cores converted
+        B = decomp.overlapped_exchange_numpy(want, L, rank, decomp.TorchTransport(dist))
         # the error/MaxLambda reductions of an advance (sum of counters, max of bits)
         import torch
         errs = torch.tensor([0, rank + 1, 0, 0, 0], dtype=torch.int32)
@@ -98,7 +101,8 @@ def _worker(rank, world, port, N, dims, q):
         tr = decomp.TorchTransport(dist)
         tr.sum_(errs)
         tr.max_(bits)
-        q.put((rank, bool(np.array_equal(A, want)), errs.tolist(), float(bits.numpy().view(np.float64)[0])))
+        q.put((rank, bool(np.array_equal(A, want)) and bool(np.array_equal(B, want)), errs.tolist(),
+               float(bits.numpy().view(np.float64)[0])))
     finally:
         dist.destroy_process_group()
 
@@ -125,3 +129,11 @@ def test_gloo_exchange_reproduces_the_periodic_fill(N, dims):
         assert ok, rank
         assert errs == [0, world * (world + 1) // 2, 0, 0, 0]
         assert ml == 0.5 + world - 1
+
+
+def test_shell_mask_is_the_zones_within_ng_of_a_split_face():
+    m = decomp.shell_mask((10, 8, 7), [0])
+    assert m[:NG].all() and m[-NG:].all() and not m[NG:-NG].any()
+    m = decomp.shell_mask((10, 8, 7), [1, 2])
+    assert m[:, :NG].all() and m[:, :, -NG:].all() and not m[:, NG:-NG, NG:-NG].any()
+    assert decomp.shell_mask((5, 8, 8), [0]).all()      # thinner than 2 Ng: all shell

@@ -1,5 +1,6 @@
-"""The decomposed advance on one GPU: every rank's block in this process (one stream, slabs
-copied directly), phase by phase with the guard exchange between c2p and the sweeps --
+"""The decomposed advance on one GPU: every rank's block in this process (the blocks' stream
+plus a side stream for the slabs, copied directly), phase by phase with the guard exchange
+between c2p and the sweeps -- overlapped with the cores' c2p, or after the whole c2p --
 against the single-box solver of the whole domain.  Power-of-two boxes on the unit cube keep
 each block's spacing (local extent / local zones, as the reference's decomposed domain
 computes it) bitwise equal to the whole box's, so the comparison is exact."""
@@ -22,9 +23,9 @@ def single(scheme, n, P0, dts):
     return out, errs
 
 
-def decomposed(scheme, n, dims, P0, dts):
+def decomposed(scheme, n, dims, P0, dts, overlap=True):
     L = Layout(N=n, dims=dims, x0=(0.0,) * len(n), x1=(1.0,) * len(n))
-    D = DecomposedSolver(scheme, L, ranks=range(dims[0] * dims[1] * dims[2]))
+    D = DecomposedSolver(scheme, L, ranks=range(dims[0] * dims[1] * dims[2]), overlap=overlap)
     D.upload_global(P0)
     D.advance(dt=0.0)
     errs = [D.errors()]
@@ -35,9 +36,10 @@ def decomposed(scheme, n, dims, P0, dts):
     return D, out, errs
 
 
+@pytest.mark.parametrize("overlap", [True, False])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("dims", [(2, 1, 1), (1, 2, 1), (2, 2, 1), (1, 2, 2), (2, 2, 2)])
-def test_decomposed_3d_matches_the_whole_box(dims, precision):
+def test_decomposed_3d_matches_the_whole_box(dims, precision, overlap):
     n = (16, 16, 16)
     scheme = Scheme(extrap="plm", riemann="hlld", advance="rk2", precision=precision)
     P0 = ics.turbulence_box(n, seed=81)
@@ -47,7 +49,7 @@ def test_decomposed_3d_matches_the_whole_box(dims, precision):
     dt = s.get_timestep(0.3)
     s.close()
     ref, e1 = single(scheme, n, P0, [dt] * 4)
-    D, got, e2 = decomposed(scheme, n, dims, P0, [dt] * 4)
+    D, got, e2 = decomposed(scheme, n, dims, P0, [dt] * 4, overlap)
     assert e1 == e2 == [0] * 5
     assert np.array_equal(got, ref), np.abs(got - ref).max()
     D.close()

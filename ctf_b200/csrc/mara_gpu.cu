@@ -981,7 +981,6 @@ int mgpu_advance_phase(mgpu_solver *h, int phase, int stage, int dt_mode, double
   if (phase < 0 || phase > 5 || stage < 0 || stage > ns || ((phase == 2 || phase >= 4) && stage >= ns) ||
       (dt_mode != 0 && dt_mode != 1))
     return fail(h, MGPU_ERR_ARG, "bad advance phase arguments");
-  if (phase >= 4 && lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   AdvanceArgs A;
   A.g = h->g;
   A.pp = phys(h);
@@ -1026,7 +1025,6 @@ int mgpu_set_external_guards(mgpu_solver *h, const int *ext, const int *mult)
   if (total > 0 && !mult) return fail(h, MGPU_ERR_ARG, "external guards need multiplicity tables");
   if (total > 0 && h->cfg.godunov != MGPU_GODUNOV_PLM_SPLIT)
     return fail(h, MGPU_ERR_UNSUPPORTED, "the CTU-Hancock operator runs on single domains only");
-  if (total > 0 && lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
   for (long long i = 0; i < total; ++i)
     if (mult[i] < 1) return fail(h, MGPU_ERR_ARG, "multiplicities must be >= 1");
   if (h->mult) cudaFree(h->mult);
@@ -1069,7 +1067,8 @@ static int halo(mgpu_solver *h, int which, int dim, int side, void *buf, int pac
   if (rc) return rc;
   if (!buf || dim < 0 || dim >= h->g.nd || (which != 0 && which != 1) || (side != 0 && side != 1))
     return fail(h, MGPU_ERR_ARG, "bad halo arguments");
-  if (lean(h)) return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout runs on single domains only");
+  if (lean(h) && which == 1)   // the lean layout's committed state is PA (which 0) and U[cur]
+    return fail(h, MGPU_ERR_UNSUPPORTED, "the lean layout exchanges its stage primitives only (which 0)");
   TransferArgs t = transfer_args(h);
   if (use_stream) t.stream = stream;
   if (which == 1) {

@@ -101,6 +101,16 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
     k_begin<<<1, 32, 0, st>>>(A.ctl, A.dt_mode, A.dt, A.cfl, A.min_dx);
   } else if (phase == PH_C2P) {
     if (s > 0) c2p(s == ns ? C2P_LEAN_CLOSING : C2P_LEAN_STAGE, 0, learned);
+  } else if (phase == PH_C2P_SHELL || phase == PH_C2P_CORE) {
+    // a stage's c2p by region (decomposed blocks); the first stage has none
+    if (s == 0) return cudaGetLastError();
+    if (learned) {
+      if (phase == PH_C2P_SHELL) c2p(C2P_LEAN_STAGE, 0, true);
+      return cudaGetLastError();
+    }
+    ProfScope ps(pr, st, KC_C2P, g.ninterior);
+    k_cons_to_prim_region<T><<<cgrid, 128, 0, st>>>(g, none, PA, UA, UB, A.pp, A.ctl, s, 0, C2P_LEAN_STAGE, A.ereset,
+                                                     A.preset, A.dreset, phase == PH_C2P_SHELL ? 1 : 2);
   } else if (phase == PH_FLUX_UPDATE) {
     const StageKind kind = stage_kind(A.rk, s);
     const LeanCombine c = lean_combine(kind.combine);

@@ -279,7 +279,9 @@ inline unsigned lean_ct_tiles(const Grid &g)
 
 // ---- host <-> lean committed state ---------------------------------------------------------------
 // Upload of a range of zones of the AoS primitives: each interior zone goes to PA and its
-// periodic images, P->U of its FP64 primitives to U[cur] (field to the images too); guard
+// periodic images (along the dimensions this grid fills itself; a decomposed block's split
+// dimensions get their guards from the exchange), P->U of its FP64 primitives to U[cur]
+// (field to the images too); guard
 // zones of the range are skipped (their images come from the interior zones, as the
 // reference's PrimToCons fills guards before converting, Mara/hydro.cpp:112-123).
 template <class T>
@@ -300,9 +302,9 @@ __global__ void k_lean_upload(Grid g, const double *__restrict__ aos, long long 
 #pragma unroll
   for (int q = 0; q < 5; ++q) U.bulk[q * g.cs + z] = T(u[q]);
   int pi[3], pj[3], pk[3];
-  const int ni = images_1d(i, g.n[0], g.ng, true, pi);
-  const int nj = images_1d(j, g.n[1], g.ng, true, pj);
-  const int nk = images_1d(k, g.n[2], g.ng, true, pk);
+  const int ni = images_1d(i, g.n[0], g.ng, self_periodic(g, 0), pi);
+  const int nj = images_1d(j, g.n[1], g.ng, self_periodic(g, 1), pj);
+  const int nk = images_1d(k, g.n[2], g.ng, self_periodic(g, 2), pk);
   for (int a = 0; a < ni; ++a)
     for (int b = 0; b < nj; ++b)
       for (int c = 0; c < nk; ++c) {

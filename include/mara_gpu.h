@@ -64,7 +64,8 @@ typedef struct {
                           (a 1024^3 FP32-bulk box): the sweeps add their flux differences
                           straight into the Runge-Kutta register and only the six transverse
                           face fields are stored (144 B per zone in FP32 bulk, 240 B in FP64).
-                          Lean needs nd = 3, 'plm-split', rk 1-3 and a single domain; results
+                          Lean needs nd = 3, 'plm-split' and rk 1-3 (decomposed blocks
+                          exchange their stage primitives, which 0, every stage); results
                           agree with the standard layout to the bulk type's rounding, the
                           magnetic field and its divergence stay FP64 as there; after a failed
                           advance the primitives are the c2p of the unchanged conserved state;

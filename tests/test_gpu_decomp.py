@@ -55,6 +55,46 @@ def test_decomposed_3d_matches_the_whole_box(dims, precision, overlap):
     D.close()
 
 
+@pytest.mark.parametrize("dims", [(2, 1, 1), (1, 2, 2), (2, 2, 2)])
+@pytest.mark.parametrize("learned", [False, True])
+def test_decomposed_lean_layout_matches_the_whole_box(dims, learned):
+    """The lean layout (FP32 bulk; the layout of the 1024^3 boxes) decomposed: each block's
+    stage primitives get their split guards from the exchange at every stage (the first
+    stage's are the committed ones), the corner EMFs read the face fields of one halo row, and
+    the blocks together give the whole lean box bit for bit, MaxLambda included."""
+    from ctf_b200.train_c2p import load as load_net
+    n = (16, 16, 16)
+    scheme = Scheme(extrap="weno5", riemann="hlld", advance="rk3", precision="fp32", layout="lean",
+                    learned_c2p=learned)
+    P0 = ics.turbulence_box(n, seed=84)
+    s = Solver(scheme, n)
+    if learned:
+        s.set_c2p_network(load_net())
+    s.upload(P0.copy())
+    assert s.advance(0.0) == 0
+    dt = s.get_timestep(0.3)
+    errs = [s.advance(dt) for _ in range(3)]
+    ml = s.max_lambda
+    ref = s.download()
+    s.close()
+    L = Layout(N=n, dims=dims, x0=(0.0,) * 3, x1=(1.0,) * 3)
+    D = DecomposedSolver(scheme, L, ranks=range(dims[0] * dims[1] * dims[2]))
+    if learned:
+        for b in D.blocks:
+            b.solver.set_c2p_network(load_net())
+    D.upload_global(P0)
+    D.advance(dt=0.0)
+    assert D.errors() == 0
+    for _ in range(3):
+        D.advance(dt=dt)
+        assert D.errors() == 0
+    assert errs == [0, 0, 0]
+    got = D.download_global()
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+    assert all(b.solver.max_lambda == ml for b in D.blocks)
+    D.close()
+
+
 def test_decomposed_2d_weno5_hllc_rk3():
     n = (32, 16)
     scheme = Scheme(extrap="weno5", riemann="hllc", advance="rk3")

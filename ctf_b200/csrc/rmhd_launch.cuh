@@ -119,7 +119,8 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
       launch_lean_sweep<T>(g, d, A.pp.riemann, st, PA, UA, UB, Bf, c, A.pp, A.ctl, s);
     }
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
-    k_lean_ct_tiled<T><<<lean_ct_tiles(g), CT_TI * CT_TJ * CT_TK, 0, st>>>(
+    const unsigned zb = 256;
+    k_lean_ct<T><<<(unsigned) ((g.ninterior + zb - 1) / zb), zb, 0, st>>>(
         g, kind.combine, UA, UB, Bf, A.ctl, s, make_double3(1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz));
   } else if (phase == PH_COMMIT) {
     {

@@ -11,7 +11,7 @@
 // No hydrodynamic face flux is stored: each sweep adds its flux differences to the register,
 //   U1 = alpha U0 + beta U1 + gamma dt L,
 // the x sweep with the combine, the y and z sweeps with += gamma dt L_d, and the field is
-// updated by k_lean_ct_tiled from Bf afterwards (Mara/rmhd.cpp:311-381, Mara/runge-kutta.hpp).
+// updated by k_lean_ct from Bf afterwards (Mara/rmhd.cpp:311-381, Mara/runge-kutta.hpp).
 //
 // One advance: begin | per stage: c2p of U[!cur] -> PA (skipped at stage 1, where PA already
 // holds the primitives of U[cur]) | sweeps x, y, z | CT | closing c2p of U[!cur] -> PA, and
@@ -197,59 +197,35 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
 }
 
 // ---- flux-CT of the field from Bf, FP64 (ConstrainedTransport3d, Mara/rmhd.cpp:311-381) ------
-// The field update of a stage: U1.B = combine(U0.B, U1.B, dt L), L the divergence of the twelve
-// corner EMFs around the zone (2 F0 + F[+b] + F[-b] - G0 - G[+a] - G[-b] - G[+a-b]) / 8, F the
-// a-face field of B_b and G the b-face field of B_a, the zeroed normal fluxes dropped and 1/dx
-// taken from the host.  A CTA takes a tile of CT_TI x CT_TJ x CT_TK interior zones, loads the
-// six face fields of the tile and a one-zone halo around it once (coalesced rows along k, each
-// value widened to FP64 once), and every zone then reads its EMFs' 84 operands from shared
-// memory instead of from L1/L2.  Zones of a partial tile past the interior load clamped
-// (in-grid) operands and store nothing.
-constexpr int CT_TI = 2, CT_TJ = 4, CT_TK = 32;
-constexpr int CT_HI = CT_TI + 2, CT_HJ = CT_TJ + 2, CT_HK = CT_TK + 2;
-constexpr int CT_CELLS = CT_HI * CT_HJ * CT_HK;
-
-__device__ __forceinline__ double ct_emf_s(const double *F, const double *G, int c, int sa, int sb)
+template <class T>
+__device__ __forceinline__ double lean_emf(const T *F, const T *G, long long z, long long sa, long long sb)
 {
-  return (2 * F[c] + F[c + sb] + F[c - sb] - G[c] - G[c + sa] - G[c - sb] - G[c + sa - sb]) * 0.125;
+  return (2 * double(F[z]) + double(F[z + sb]) + double(F[z - sb]) - double(G[z]) - double(G[z + sa]) -
+          double(G[z - sb]) - double(G[z + sa - sb])) * 0.125;
 }
 
 template <class T>
-__global__ void __launch_bounds__(CT_TI * CT_TJ * CT_TK) k_lean_ct_tiled(Grid g, int combine, StatePtr<T> UA,
-                                                                        StatePtr<T> UB, const T *__restrict__ Bf,
-                                                                        const Ctl *ctl, int stage, double3 inv)
+__global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int combine, StatePtr<T> UA, StatePtr<T> UB,
+                                                                   const T *__restrict__ Bf, const Ctl *ctl,
+                                                                   int stage, double3 inv)
 {
   if (stage_failed(ctl, stage + 1)) return;
-  __shared__ double sf[6][CT_CELLS];
-  const int nbk = (g.n[2] + CT_TK - 1) / CT_TK, nbj = (g.n[1] + CT_TJ - 1) / CT_TJ;
-  const int bk = blockIdx.x % nbk;
-  const int bj = (blockIdx.x / nbk) % nbj;
-  const int bi = blockIdx.x / (nbk * nbj);
-  const int i0 = g.ng + bi * CT_TI - 1, j0 = g.ng + bj * CT_TJ - 1, k0 = g.ng + bk * CT_TK - 1;   // halo corner
-  for (int c = threadIdx.x; c < CT_CELLS; c += blockDim.x) {
-    const int ci = c / (CT_HJ * CT_HK), cj = (c / CT_HK) % CT_HJ, ck = c % CT_HK;
-    const int i = min(i0 + ci, g.G[0] - 1), j = min(j0 + cj, g.G[1] - 1), k = min(k0 + ck, g.G[2] - 1);
-    const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) sf[f][c] = double(Bf[(long long) f * g.cs + z]);
-  }
-  __syncthreads();
-  const int ti = threadIdx.x / (CT_TJ * CT_TK), tj = (threadIdx.x / CT_TK) % CT_TJ, tk = threadIdx.x % CT_TK;
-  const int i = g.ng + bi * CT_TI + ti, j = g.ng + bj * CT_TJ + tj, k = g.ng + bk * CT_TK + tk;
-  if (i >= g.ng + g.n[0] || j >= g.ng + g.n[1] || k >= g.ng + g.n[2]) return;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ninterior) return;
   StatePtr<T> U0, U1;
   lean_regs(ctl, UA, UB, U0, U1);
-  const long long z = ((long long) i * g.G[1] + j) * g.G[2] + k;
-  const int c = ((ti + 1) * CT_HJ + (tj + 1)) * CT_HK + (tk + 1);
-  const int sx = CT_HJ * CT_HK, sy = CT_HK, sz = 1;
-  const double *xBy = sf[0], *xBz = sf[1], *yBx = sf[2], *yBz = sf[3], *zBx = sf[4], *zBy = sf[5];
-  const double FxBy0 = ct_emf_s(xBy, yBx, c, sx, sy), FxBym = ct_emf_s(xBy, yBx, c - sx, sx, sy);
-  const double FyBx0 = ct_emf_s(yBx, xBy, c, sy, sx), FyBxm = ct_emf_s(yBx, xBy, c - sy, sy, sx);
-  const double FyBz0 = ct_emf_s(yBz, zBy, c, sy, sz), FyBzm = ct_emf_s(yBz, zBy, c - sy, sy, sz);
-  const double FzBy0 = ct_emf_s(zBy, yBz, c, sz, sy), FzBym = ct_emf_s(zBy, yBz, c - sz, sz, sy);
-  const double FzBx0 = ct_emf_s(zBx, xBz, c, sz, sx), FzBxm = ct_emf_s(zBx, xBz, c - sz, sz, sx);
-  const double FxBz0 = ct_emf_s(xBz, zBx, c, sx, sz), FxBzm = ct_emf_s(xBz, zBx, c - sx, sx, sz);
+  const long long z = interior_zone(g, t);
+  const long long sx = g.s[0], sy = g.s[1], sz = g.s[2];
+  const T *xBy = Bf + 0 * g.cs, *xBz = Bf + 1 * g.cs, *yBx = Bf + 2 * g.cs, *yBz = Bf + 3 * g.cs,
+          *zBx = Bf + 4 * g.cs, *zBy = Bf + 5 * g.cs;
+  const double FxBy0 = lean_emf(xBy, yBx, z, sx, sy), FxBym = lean_emf(xBy, yBx, z - sx, sx, sy);
+  const double FyBx0 = lean_emf(yBx, xBy, z, sy, sx), FyBxm = lean_emf(yBx, xBy, z - sy, sy, sx);
+  const double FyBz0 = lean_emf(yBz, zBy, z, sy, sz), FyBzm = lean_emf(yBz, zBy, z - sy, sy, sz);
+  const double FzBy0 = lean_emf(zBy, yBz, z, sz, sy), FzBym = lean_emf(zBy, yBz, z - sz, sz, sy);
+  const double FzBx0 = lean_emf(zBx, xBz, z, sz, sx), FzBxm = lean_emf(zBx, xBz, z - sz, sz, sx);
+  const double FxBz0 = lean_emf(xBz, zBx, z, sx, sz), FxBzm = lean_emf(xBz, zBx, z - sx, sx, sz);
   double Lb[3];
+  // the zeroed normal fluxes drop out; 1/dx from the host instead of six FP64 divisions
   Lb[0] = -(FyBx0 - FyBxm) * inv.y - (FzBx0 - FzBxm) * inv.z;
   Lb[1] = -(FxBy0 - FxBym) * inv.x - (FzBy0 - FzBym) * inv.z;
   Lb[2] = -(FxBz0 - FxBzm) * inv.x - (FyBz0 - FyBzm) * inv.y;
@@ -266,12 +242,6 @@ __global__ void __launch_bounds__(CT_TI * CT_TJ * CT_TK) k_lean_ct_tiled(Grid g,
     }
     U1.B[q * g.cs + z] = out;
   }
-}
-
-inline unsigned lean_ct_tiles(const Grid &g)
-{
-  return (unsigned) ((long long) ((g.n[0] + CT_TI - 1) / CT_TI) * ((g.n[1] + CT_TJ - 1) / CT_TJ) *
-                     ((g.n[2] + CT_TK - 1) / CT_TK));
 }
 
 // ---- commit of the lean layout ------------------------------------------------------------------

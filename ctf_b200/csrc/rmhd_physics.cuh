@@ -17,7 +17,6 @@
 //   HLLC         Mara/riemann_hllc-rmhd.cpp:26-178
 //   HLLD         Mara/riemann_hlld-rmhd.cpp:179-615, Newton Mara/nrsolver.cpp:89-152
 #pragma once
-#include <type_traits>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -1266,29 +1265,12 @@ __device__ __forceinline__ T hlld_estimate1(T E, T FE, T m, T Fm)
   return (p1 < p2) ? p1 : p2;
 }
 
-// The face states the HLLC fallback of riemann_hlld starts from: by default a copy of the
-// ones riemann_hlld was given, which then stay live through the whole pressure iteration; a
-// caller that can rebuild them (reconstruct again from the stage primitives) passes a functor
-// that writes them, and holds no copy meanwhile.
-template <class T>
-struct KeepFaceStates {
-  const T *pl, *pr;
-  __device__ void operator()(T *a, T *b) const
-  {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      a[i] = pl[i];
-      b[i] = pr[i];
-    }
-  }
-};
-
 // HlldRmhdRiemannSolver::IntercellFlux at s = 0 (riemann_hlld-rmhd.cpp:179-313).
 // Returns 1 when a face state is unphysical (the caller retries with PCM states);
 // `used_hllc` reports the fallback.
-template <class T, int dim, class Reload = KeepFaceStates<T>>
+template <class T, int dim>
 __device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, const T *pr, T *f, T &ml,
-                                         int &used_hllc, C2PTally *tally, const Reload &reload = Reload{})
+                                         int &used_hllc, C2PTally *tally)
 {
   using Tol = RmhdTol<T>;
   const T gamma = T(pp.gamma);
@@ -1389,12 +1371,8 @@ __device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, c
   }
   used_hllc = 1;
   Face8<T> a, b;
-  if constexpr (std::is_same<Reload, KeepFaceStates<T>>::value) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) { a.v[i] = pl[i]; b.v[i] = pr[i]; }
-  } else {
-    reload(a.v, b.v);
-  }
+  for (int i = 0; i < 8; ++i) { a.v[i] = pl[i]; b.v[i] = pr[i]; }
   const HllcOut<T> o = riemann_hllc_fallback<T, dim>(gamma, a, b, ml);
   ml = o.ml;
 #pragma unroll

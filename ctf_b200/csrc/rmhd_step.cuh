@@ -177,6 +177,7 @@ __device__ __forceinline__ void c2p_finish(const Grid &g, T *PA, StatePtr<T> Pn,
     warp_add(&st.c2p_calls, 1u);
     warp_add(&st.c2p_iters, (unsigned) tally.iters);
     if (tally.attempts >= 1 && tally.attempts <= 5) warp_add(&st.c2p_attempt[tally.attempts], 1u);
+    warp_add(&st.c2p_failed, err ? 1u : 0u);
   }
   if (err) {
     if (ereset) {   // emergency reset of the failed zone
@@ -332,28 +333,24 @@ __device__ __forceinline__ void face_flux(const Grid &g, const T *__restrict__ P
                                           T &ml, FluxTally &ft, T *Fo)
 {
   const long long S = g.s[dim - 1];
+  T Pl[8], Pr[8];
   const T theta = T(pp.theta);
-  // The face states of attempt 0 (reconstructed) and attempt 1 (the zone states themselves,
-  // the PCM retry).  HLLD takes this as its way to rebuild the states for its HLLC fallback
-  // instead of holding a copy through its pressure iteration.
-  const auto states = [&](int attempt, T *Pl, T *Pr) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const T *a = PA + q * g.cs + f;
-      if (attempt == 1 || pp.recon == RECON_PCM) {
-        Pl[q] = a[0];
-        Pr[q] = a[S];
-      } else if (pp.recon == RECON_PLM) {
-        const T vm = a[-S], v0 = a[0], vp = a[S], vpp = a[2 * S];
-        Pl[q] = plm(theta, vm, v0, vp, T(+1));
-        Pr[q] = plm(theta, v0, vp, vpp, T(-1));
-      } else {
-        const T vm2 = a[-2 * S], vm1 = a[-S], v0 = a[0], vp1 = a[S], vp2 = a[2 * S], vp3 = a[3 * S];
-        Pl[q] = weno5(pp.is_mode, T(pp.sz10A), vm2, vm1, v0, vp1, vp2, true);
-        Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
-      }
+  for (int q = 0; q < 8; ++q) {
+    const T *a = PA + q * g.cs + f;
+    if (pp.recon == RECON_PCM) {
+      Pl[q] = a[0];
+      Pr[q] = a[S];
+    } else if (pp.recon == RECON_PLM) {
+      const T vm = a[-S], v0 = a[0], vp = a[S], vpp = a[2 * S];
+      Pl[q] = plm(theta, vm, v0, vp, T(+1));
+      Pr[q] = plm(theta, v0, vp, vpp, T(-1));
+    } else {
+      const T vm2 = a[-2 * S], vm1 = a[-S], v0 = a[0], vp1 = a[S], vp2 = a[2 * S], vp3 = a[3 * S];
+      Pl[q] = weno5(pp.is_mode, T(pp.sz10A), vm2, vm1, v0, vp1, vp2, true);
+      Pr[q] = weno5(pp.is_mode, T(pp.sz10A), vm1, v0, vp1, vp2, vp3, false);
     }
-  };
+  }
   const T gamma = T(pp.gamma);
   int err = 1, used_hllc = 0;
   constexpr bool hlld = RS == RIEMANN_HLLD;
@@ -362,22 +359,18 @@ __device__ __forceinline__ void face_flux(const Grid &g, const T *__restrict__ P
   // One call site per solver keeps a single inlined copy of it.
 #pragma unroll 1
   for (int attempt = 0; attempt < 2 && err; ++attempt) {
-    if (attempt == 1) ft.pcm_retry += 1;
-    T Pl[8], Pr[8];
-    states(attempt, Pl, Pr);
-    C2PTally t{0, 0};
-    if constexpr (RS == RIEMANN_HLLD) {
-      if constexpr (sizeof(T) < sizeof(double)) {
-        const auto reload = [&](T *a, T *b) { states(attempt, a, b); };
-        err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t, reload);
-      } else {
-        err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
+    if (attempt == 1) {
+      ft.pcm_retry += 1;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        Pl[q] = PA[q * g.cs + f];
+        Pr[q] = PA[q * g.cs + f + S];
       }
-    } else if constexpr (RS == RIEMANN_HLLC) {
-      err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
-    } else {
-      err = riemann_hll<T, dim>(gamma, Pl, Pr, Fo, ml);
     }
+    C2PTally t{0, 0};
+    if constexpr (RS == RIEMANN_HLLD) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
+    else if constexpr (RS == RIEMANN_HLLC) err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
+    else err = riemann_hll<T, dim>(gamma, Pl, Pr, Fo, ml);
     tally.iters += t.iters;
     tally.attempts += t.attempts;
   }

@@ -91,7 +91,7 @@ CFL = 0.3
 # (dram__bytes_read.sum + dram__bytes_write.sum) per work unit, and the issue/pipe
 # utilisation that bounds the lean HLLD sweeps.  They come from separate captures, not from
 # the run that prints them.
-NCU_TRAFFIC_PER_UNIT = {}
+NCU_TRAFFIC_PER_UNIT = {("update", "plm", "hlld", "lean"): 69.7}   # a first-stage CT launch
 NCU_LIMITER = {
     ("flux", "weno5", "hlld", "lean"): {"issue_active": 0.467, "fma_pipe": 0.281, "xu_pipe": 0.194,
                                         "dram_throughput": 0.068},

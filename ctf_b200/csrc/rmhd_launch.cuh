@@ -120,7 +120,7 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
     }
     ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
     const unsigned zb = 256;
-    k_lean_ct<T><<<(unsigned) ((g.ninterior + zb - 1) / zb), zb, 0, st>>>(
+    k_lean_ct<T><<<(unsigned) ((lean_ct_threads(g) + zb - 1) / zb), zb, 0, st>>>(
         g, kind.combine, UA, UB, Bf, A.ctl, s, make_double3(1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz));
   } else if (phase == PH_COMMIT) {
     {

@@ -204,17 +204,12 @@ __device__ __forceinline__ double lean_emf(const T *F, const T *G, long long z, 
           double(G[z - sb]) - double(G[z + sa - sb])) * 0.125;
 }
 
+// The field update of one interior zone z: U1.B = combine(U0.B, U1.B, dt L), L the divergence
+// of the twelve corner EMFs around it (the zeroed normal fluxes dropped, 1/dx from the host).
 template <class T>
-__global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int combine, StatePtr<T> UA, StatePtr<T> UB,
-                                                                   const T *__restrict__ Bf, const Ctl *ctl,
-                                                                   int stage, double3 inv)
+__device__ __forceinline__ void lean_ct_zone(const Grid &g, int combine, StatePtr<T> U0, StatePtr<T> U1,
+                                             const T *__restrict__ Bf, double dtd, double3 inv, long long z)
 {
-  if (stage_failed(ctl, stage + 1)) return;
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
-  StatePtr<T> U0, U1;
-  lean_regs(ctl, UA, UB, U0, U1);
-  const long long z = interior_zone(g, t);
   const long long sx = g.s[0], sy = g.s[1], sz = g.s[2];
   const T *xBy = Bf + 0 * g.cs, *xBz = Bf + 1 * g.cs, *yBx = Bf + 2 * g.cs, *yBz = Bf + 3 * g.cs,
           *zBx = Bf + 4 * g.cs, *zBy = Bf + 5 * g.cs;
@@ -225,11 +220,9 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int c
   const double FzBx0 = lean_emf(zBx, xBz, z, sz, sx), FzBxm = lean_emf(zBx, xBz, z - sz, sz, sx);
   const double FxBz0 = lean_emf(xBz, zBx, z, sx, sz), FxBzm = lean_emf(xBz, zBx, z - sx, sx, sz);
   double Lb[3];
-  // the zeroed normal fluxes drop out; 1/dx from the host instead of six FP64 divisions
   Lb[0] = -(FyBx0 - FyBxm) * inv.y - (FzBx0 - FzBxm) * inv.z;
   Lb[1] = -(FxBy0 - FxBym) * inv.x - (FzBy0 - FzBym) * inv.z;
   Lb[2] = -(FxBz0 - FxBzm) * inv.x - (FyBz0 - FyBzm) * inv.y;
-  const double dtd = ctl->dt;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const double un = U0.B[q * g.cs + z];
@@ -243,6 +236,33 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int c
     U1.B[q * g.cs + z] = out;
   }
 }
+
+// Two zones per thread, neighbours along the contiguous axis: their EMF stencils share most
+// operands (and two EMFs: zone k+1's lower z-EMFs are zone k's upper ones), which the compiler
+// loads and widens once.  Each zone's arithmetic is lean_ct_zone's.
+template <class T>
+__global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int combine, StatePtr<T> UA, StatePtr<T> UB,
+                                                                   const T *__restrict__ Bf, const Ctl *ctl,
+                                                                   int stage, double3 inv)
+{
+  if (stage_failed(ctl, stage + 1)) return;
+  const long long npair = (g.n[2] + 1) / 2;
+  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long) g.n[0] * g.n[1] * npair) return;
+  StatePtr<T> U0, U1;
+  lean_regs(ctl, UA, UB, U0, U1);
+  const int kp = (int) (t % npair);
+  const long long ij = t / npair;
+  const int j = (int) (ij % g.n[1]), i = (int) (ij / g.n[1]);
+  const int k = 2 * kp;
+  const long long z = ((long long) (i + g.ng) * g.G[1] + (j + g.ng)) * g.G[2] + (k + g.ng);
+  const double dtd = ctl->dt;
+  lean_ct_zone<T>(g, combine, U0, U1, Bf, dtd, inv, z);
+  if (k + 1 < g.n[2]) lean_ct_zone<T>(g, combine, U0, U1, Bf, dtd, inv, z + 1);
+}
+
+// Threads of k_lean_ct for a grid (two zones along k each).
+inline long long lean_ct_threads(const Grid &g) { return (long long) g.n[0] * g.n[1] * ((g.n[2] + 1) / 2); }
 
 // ---- commit of the lean layout ------------------------------------------------------------------
 // As k_commit, then the restore c2p (C2P_LEAN_RESTORE) runs when nothing was committed.

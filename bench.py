@@ -58,6 +58,8 @@ WORKLOADS = {
                                dict(extrap="weno5", riemann="hlld", advance="rk3")),
     "turb160_plm_hlld_rk3": ((160, 160, 160), "turbulence",
                              dict(extrap="plm", riemann="hlld", advance="rk3")),
+    "turb256_plm_hlld_rk3": ((256, 256, 256), "turbulence",
+                             dict(extrap="plm", riemann="hlld", advance="rk3")),
     # the high-magnetisation stress box (W log-uniform in [1, 10], sigma log-uniform in
     # [0.1, 10], p = 0.01): the reference's algorithm fails its first step, so it runs with the
     # reference's emergency reset (config_solver{ereset = true, preset = 0.01, dreset = 1})
@@ -91,8 +93,13 @@ CFL = 0.3
 # (dram__bytes_read.sum + dram__bytes_write.sum) per work unit, and the issue/pipe
 # utilisation that bounds the lean HLLD sweeps.  They come from separate captures, not from
 # the run that prints them.
-NCU_TRAFFIC_PER_UNIT = {("update", "plm", "hlld", "lean"): 69.7}   # a first-stage CT launch
+NCU_TRAFFIC_PER_UNIT = {("update", "plm", "hlld", "lean"): 69.7,    # a first-stage CT launch
+                        # the x sweep's DRAM bytes per zone, 120.2 against its 100 algorithmic,
+                        # applied as that 1.202 ratio to the mean of the three sweeps (86.7 B)
+                        ("flux", "plm", "hlld", "lean"): 104.2}
 NCU_LIMITER = {
+    ("flux", "plm", "hlld", "lean"): {"issue_active": 0.507, "fma_pipe": 0.263, "xu_pipe": 0.133,
+                                      "dram_throughput": 0.086},
     ("flux", "weno5", "hlld", "lean"): {"issue_active": 0.467, "fma_pipe": 0.281, "xu_pipe": 0.194,
                                         "dram_throughput": 0.068},
     ("flux", "weno5", "hlld", "standard"): {"issue_active": 0.500, "fma_pipe": 0.292, "xu_pipe": 0.210},

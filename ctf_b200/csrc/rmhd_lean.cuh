@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
   __shared__ T flo[128][5];   // the carried lower-face flux of each thread
+  __shared__ HlldSlot<T> hslot[RS == RIEMANN_HLLD && sizeof(T) < sizeof(double) ? 128 : 1];
   if (t < ncol * nchunk) {
     const int chunk = (int) (t / ncol);
     const long long col = t - (long long) chunk * ncol;
@@ -130,7 +131,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
         }
       }
       T Fo[8];
-      face_flux<T, dim, RS>(g, PA, pp, f, ml, ft, Fo);
+      face_flux<T, dim, RS>(g, PA, pp, f, ml, ft, Fo,
+                            RS == RIEMANN_HLLD && sizeof(T) < sizeof(double) ? &hslot[threadIdx.x] : nullptr);
       if (m >= m0 || chunk == 0) {            // the chunk's first face is its neighbour's last
         slot0[f] = Fo[dim == 1 ? By : Bx];
         slot1[f] = Fo[Bz];
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
   __shared__ T fs[5][128];
+  __shared__ HlldSlot<T> hslot[RS == RIEMANN_HLLD && sizeof(T) < sizeof(double) ? 128 : 1];
   const bool active = q >= 0 && q < total;
   long long f = 0;
   bool upd = false;
@@ -174,7 +177,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
 #pragma unroll
     for (int r = 0; r < 5; ++r) asm volatile("prefetch.global.L2 [%0];" ::"l"(U1.bulk + r * g.cs + f));
     T Fo[8];
-    face_flux<T, 3, RS>(g, PA, pp, f, ml, ft, Fo);
+    face_flux<T, 3, RS>(g, PA, pp, f, ml, ft, Fo,
+                        RS == RIEMANN_HLLD && sizeof(T) < sizeof(double) ? &hslot[threadIdx.x] : nullptr);
     if (threadIdx.x > 0 || blockIdx.x == 0) {
       Bf[(long long) bf_slot(3, Bx) * g.cs + f] = Fo[Bx];
       Bf[(long long) bf_slot(3, By) * g.cs + f] = Fo[By];

@@ -1268,16 +1268,28 @@ __device__ __forceinline__ T hlld_estimate1(T E, T FE, T m, T Fm)
 // HlldRmhdRiemannSolver::IntercellFlux at s = 0 (riemann_hlld-rmhd.cpp:179-313).
 // Returns 1 when a face state is unphysical (the caller retries with PCM states);
 // `used_hllc` reports the fallback.
+// A thread's slot for the HLLD equation state in shared memory (53 words: an odd stride, so
+// the threads of a warp hit different banks).
+template <class T>
+struct HlldSlot {
+  HlldEqn<T> q;
+  T pad;
+};
+
+// slot: where the equation state lives through the pressure iteration -- nullptr for
+// registers (the compiler's choice), or this thread's HlldSlot in shared memory, so that the
+// ~50 values are read from there when needed instead of occupying registers throughout.
 template <class T, int dim>
 __device__ __forceinline__ int riemann_hlld(const PhysParams &pp, const T *pl, const T *pr, T *f, T &ml,
-                                         int &used_hllc, C2PTally *tally)
+                                         int &used_hllc, C2PTally *tally, HlldSlot<T> *slot = nullptr)
 {
   using Tol = RmhdTol<T>;
   const T gamma = T(pp.gamma);
   using M = DimMap<dim>;
   constexpr int B1 = M::B1, B2 = M::B2, B3 = M::B3, S1 = M::S1, S2 = M::S2, S3 = M::S3;
   constexpr int v1 = M::v1, v2 = M::v2, v3 = M::v3;
-  HlldEqn<T> q;
+  HlldEqn<T> q_regs;
+  HlldEqn<T> &q = slot ? slot->q : q_regs;
   T Pl[8], Pr[8], epl, eml, epr, emr;
   Pl[pre] = pl[pre]; Pr[pre] = pr[pre];
   Pl[rho] = pl[rho]; Pr[rho] = pr[rho];

@@ -330,7 +330,7 @@ struct FluxTally {
 // attempts fail); the face's |lambda| is folded into ml.
 template <class T, int dim, int RS>
 __device__ __forceinline__ void face_flux(const Grid &g, const T *__restrict__ PA, const PhysParams &pp, long long f,
-                                          T &ml, FluxTally &ft, T *Fo)
+                                          T &ml, FluxTally &ft, T *Fo, HlldSlot<T> *slot = nullptr)
 {
   const long long S = g.s[dim - 1];
   T Pl[8], Pr[8];
@@ -368,7 +368,7 @@ __device__ __forceinline__ void face_flux(const Grid &g, const T *__restrict__ P
       }
     }
     C2PTally t{0, 0};
-    if constexpr (RS == RIEMANN_HLLD) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t);
+    if constexpr (RS == RIEMANN_HLLD) err = riemann_hlld<T, dim>(pp, Pl, Pr, Fo, ml, used_hllc, &t, slot);
     else if constexpr (RS == RIEMANN_HLLC) err = riemann_hllc<T, dim>(gamma, Pl, Pr, Fo, ml);
     else err = riemann_hll<T, dim>(gamma, Pl, Pr, Fo, ml);
     tally.iters += t.iters;

@@ -156,8 +156,13 @@ __device__ __forceinline__ void cubic(T c2, T c1, T c0, T &x1, T &x2, T &x3, int
 
 // Returns (max root, min root) over the real roots of d4 x^4 + ... + d0 with the fold used
 // by FluxAndEigenvalues: start at (-1, +1), then clamp to (1, -1) if either exceeds 1.
+// MGPU_QUARTIC_INLINE: inlined at every call site (the default), or __noinline__ for one
+// shared copy (less code in the long HLLD kernels).
+#ifndef MGPU_QUARTIC_INLINE
+#define MGPU_QUARTIC_INLINE __forceinline__
+#endif
 template <class T>
-__device__ __forceinline__ void quartic_extreme_roots(T d4, T d3, T d2, T d1, T d0, T &ap, T &am)
+__device__ MGPU_QUARTIC_INLINE void quartic_extreme_roots(T d4, T d3, T d2, T d1, T d0, T &ap, T &am)
 {
   const T a3 = d3 / d4, a2 = d2 / d4, a1 = d1 / d4, a0 = d0 / d4;
   const T au2 = -a2;

@@ -59,3 +59,16 @@ def test_ghost_correction_and_linf():
     b[0, 0, 0, 1] = 9.0            # guard zone: not counted
     r = bench.rel_linf(a, b, 3)
     assert abs(r["rho"] - 0.5 / 1.5) < 1e-15 and r["pre"] == 0.0
+
+
+def test_tiled_block_is_a_window_of_the_periodic_repetition():
+    """--decompose builds each rank's block from a small turbulence box repeated periodically:
+    a block is exactly the window of the repeated box, guards included."""
+    import numpy as np
+    import bench
+    from ctf_b200 import ics
+    t = ics.turbulence_box((8, 8, 8), seed=3)
+    assert np.array_equal(bench.tiled_block(t, (0, 0, 0), (8, 8, 8)), t)
+    whole = bench.tiled_block(t, (0, 0, 0), (16, 16, 16))
+    blk = bench.tiled_block(t, (8, 0, 4), (8, 16, 4))
+    assert np.array_equal(whole[8:8 + 14, :, 4:4 + 10], blk)

@@ -972,14 +972,26 @@ def main():
             _, e = solver_fp32.advance_host(host, min(dt, dt_fixed))
             e2e_err += e
         sec = time.perf_counter() - t0
+        slabs = solver_fp32.pipeline()[1]
+        # the same calls with the slab pipeline switched off, for the record
+        solver_fp32.set_pipeline(0)
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            dt = solver_fp32.get_timestep(CFL)
+            _, e = solver_fp32.advance_host(host, min(dt, dt_fixed))
+            e2e_err += e
+        sec_plain = time.perf_counter() - t1
+        solver_fp32.set_pipeline(-1)
         if dist is not None:
-            t = torch.tensor([sec], device="cuda")
+            t = torch.tensor([sec, sec_plain], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            sec = float(t.item())
+            sec, sec_plain = float(t[0].item()), float(t[1].item())
         nbytes = int(np.prod(solver_fp32.shape)) * 8
         out["e2e"] = {"value": int(np.prod(n)) * args.steps * world / sec, "unit": UNIT,
                       "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "errors": e2e_err,
-                      "api": "mgpu_advance_host (Mara.advance(buf, dt)) + mgpu_get_timestep"}
+                      "api": "mgpu_advance_host (Mara.advance(buf, dt)) + mgpu_get_timestep",
+                      "pipeline_slabs": slabs,
+                      "value_unpipelined": int(np.prod(n)) * args.steps * world / sec_plain}
     solver_fp32.close()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -75,6 +75,9 @@ SIGNATURES = {
     "mgpu_download_prim_range": (ctypes.c_int, [_vp, _dp, ctypes.c_longlong, ctypes.c_longlong]),
     "mgpu_advance": (ctypes.c_int, [_vp, ctypes.c_double, _ip]),
     "mgpu_advance_host": (ctypes.c_int, [_vp, _dp, ctypes.c_double, _dp, _ip]),
+    "mgpu_set_pipeline": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "mgpu_get_pipeline": (ctypes.c_int, [_vp, _ip, _ip]),
+    "mgpu_pipeline_schedule": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int]),
     "mgpu_advance_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double]),
     "mgpu_synchronize": (ctypes.c_int, [_vp]),

@@ -9,6 +9,7 @@
 #include <chrono>
 #include <string>
 #include <vector>
+#include <utility>
 
 #include "../../include/mara_gpu.h"
 #include "rmhd_types.cuh"
@@ -62,8 +63,27 @@ PhysParams phys(const mgpu_solver *h)
   return p;
 }
 
+// The pipelined host advance's buffers (allocated on its first use for the current domain).
+void pipe_free(mgpu_solver *h, bool streams)
+{
+  if (h->pipe_in) cudaFree(h->pipe_in);
+  if (h->pipe_out) cudaFree(h->pipe_out);
+  if (h->pipe_guess) cudaFree(h->pipe_guess);
+  if (h->pipe_pa) cudaFree(h->pipe_pa);
+  h->pipe_in = h->pipe_out = nullptr;
+  h->pipe_guess = h->pipe_pa = nullptr;
+  h->pipe_state = 0;
+  if (!streams) return;
+  for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
+  h->pipe_ev.clear();
+  if (h->pipe_h2d) cudaStreamDestroy(h->pipe_h2d);
+  if (h->pipe_d2h) cudaStreamDestroy(h->pipe_d2h);
+  h->pipe_h2d = h->pipe_d2h = nullptr;
+}
+
 void free_buffers(mgpu_solver *h)
 {
+  pipe_free(h, false);
   for (void *p : h->allocations) cudaFree(p);
   h->allocations.clear();
   h->b = AdvanceBuffers{};
@@ -288,6 +308,7 @@ int mgpu_destroy(mgpu_solver *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   mgpu_driving_free(h);
   free_buffers(h);
+  pipe_free(h, true);
   prof_free(h);
   if (h->mlp) cudaFree(h->mlp);
   if (h->mlp_tc) cudaFree(h->mlp_tc);
@@ -563,19 +584,272 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
   return MGPU_OK;
 }
 
+// ---- the pipelined Mara.advance(buf, dt) of the lean layout -------------------------------------
+// The box is cut into S slabs of x rows.  The operations of one advance on a slab are
+//   e = 0        upload: the copy in of its rows, then k_lean_upload (P->U into the committed
+//                register, the primitives into PA)
+//   e = 2k + 1   stage k's sweeps and CT over the slab (k = 0 .. K-1)
+//   e = 2k       stage k's c2p over the slab (k = 1 .. K-1), e = 2K the closing c2p
+//   e = 2K + 1   download: the result into the device copy-out buffer, then the copy out.
+// The stages' primitives alternate between two arrays (the solver's PA and a second one), so
+// that a c2p never overwrites primitives a neighbour's sweeps still read.  A slab's sweeps
+// (e odd) may run once the operation before them has run on the slab and on both neighbouring
+// slabs (periodic in x: slab 0's images lie next to slab S-1), because they read the
+// neighbours' stage primitives up to three rows deep; a c2p or a download needs only the
+// slab's own previous operation (CT reads face fields one row beyond the slab, which the same
+// operation's sweeps compute).  Each window launch computes exactly the faces and zones of the
+// whole-box launch that fall in it, so the result is the whole-box advance's.
+// The slabs are uploaded outward from slab 0 in both directions, so that slab 0's neighbourhood
+// arrives first; after each upload the compute stream takes every operation that became ready,
+// the latest first.  The copies run on their own streams, so the copy in of later slabs and the
+// copy out of earlier ones overlap the advance.  With a pinned caller buffer the copies out
+// write it before the advance is known to commit; its original contents stay in the device
+// copy-in buffer and go back when the advance does not commit.  A pageable buffer is written
+// after the commit only (its copies would block the host thread).
+
+// Slabs of the pipelined host advance for this solver (0: run unpipelined).
+static int pipe_slab_count(const mgpu_solver *h)
+{
+  const Grid &g = h->g;
+  if (h->pipe_slabs == 0 || !lean(h) || g.nd != 3 || g.ext[0] || g.ext[1] || g.ext[2] || h->driving ||
+      h->prof_on)
+    return 0;
+  const int smax = g.n[0] / 4;   // at least 4 rows per slab: deeper than any stencil's reach
+  if (smax < 3) return 0;
+  // automatic: about 11 rows per slab (measured on a 512^3 box: 16, 24, 32, 48 and 64 slabs
+  // take 352, 324, 314, 309 and 314 ms per call; thinner slabs shorten the copy-out tail after
+  // the last copy in, thicker ones recompute fewer halo rows of face fields)
+  int S = h->pipe_slabs > 0 ? h->pipe_slabs : g.n[0] / 11;
+  if (S < 3) S = 3;
+  if (S > smax) S = smax;
+  return S;
+}
+
+// Device buffers, streams and events of the pipeline; 1 when device memory does not allow it.
+static int pipe_setup(mgpu_solver *h, int S)
+{
+  const Grid &g = h->g;
+  const bool learned = phys(h).learned && h->mlp_tc;
+  if (h->pipe_state == 0) {
+    const size_t aos = (size_t) g.nz * 8 * sizeof(double);
+    const size_t guess = learned ? (size_t) g.ninterior * sizeof(float2) : 0;
+    const size_t pa = (size_t) g.cs * 8 * (fp32(h) ? sizeof(float) : sizeof(double));
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    if (free_b < 2 * aos + pa + guess + (size_t(1) << 30)) {
+      h->pipe_state = -1;
+      return 1;
+    }
+    cudaError_t e = cudaMalloc((void **) &h->pipe_in, aos);
+    if (e == cudaSuccess) e = cudaMalloc((void **) &h->pipe_out, aos);
+    if (e == cudaSuccess) e = cudaMalloc(&h->pipe_pa, pa);
+    if (e == cudaSuccess && guess) e = cudaMalloc(&h->pipe_guess, guess);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      pipe_free(h, false);
+      h->pipe_state = -1;
+      return 1;
+    }
+    h->pipe_state = 1;
+  }
+  if (h->pipe_state < 0) return 1;
+  if (learned && !h->pipe_guess) {   // the learned c2p was switched on after the setup
+    if (cudaMalloc(&h->pipe_guess, (size_t) g.ninterior * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      return 1;
+    }
+  }
+  if (!h->pipe_h2d) CK(cudaStreamCreateWithFlags(&h->pipe_h2d, cudaStreamNonBlocking));
+  if (!h->pipe_d2h) CK(cudaStreamCreateWithFlags(&h->pipe_d2h, cudaStreamNonBlocking));
+  while ((int) h->pipe_ev.size() < 2 * S) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->pipe_ev.push_back(e);
+  }
+  return 0;
+}
+
+// The order in which the pipelined advance issues its operations: (slab, operation) pairs,
+// the uploads included, for S slabs and K Runge-Kutta stages.
+static std::vector<std::pair<int, int>> pipe_schedule(int S, int K)
+{
+  const int E = 2 * K + 2;   // operations per slab
+  std::vector<std::pair<int, int>> out;
+  std::vector<int> order, done(S, 0);
+  order.push_back(0);
+  for (int d = 1; (int) order.size() < S; ++d) {
+    order.push_back(d);
+    if ((int) order.size() < S) order.push_back(S - d);
+  }
+  auto ready = [&](int s, int e) {
+    return done[s] == e && (e % 2 == 0 || e == E - 1 || (done[(s + S - 1) % S] >= e && done[(s + 1) % S] >= e));
+  };
+  for (int u : order) {
+    out.emplace_back(u, 0);
+    done[u] = 1;
+    for (bool any = true; any;) {   // every operation that became ready, the latest first
+      any = false;
+      for (int e = E - 1; e >= 1; --e)
+        for (int s : order)
+          if (ready(s, e)) {
+            out.emplace_back(s, e);
+            done[s] = e + 1;
+            any = true;
+          }
+    }
+  }
+  return out;
+}
+
+static int pipe_advance_host(mgpu_solver *h, double *host, double dt, int S, int *errors)
+{
+  const Grid &g = h->g;
+  const int K = num_stages(h->cfg.rk);
+  const int E = 2 * K + 2;   // operations per slab
+  const long long s0 = g.s[0], row_bytes = s0 * 8 * (long long) sizeof(double);
+  const int G0 = g.G[0], ng = g.ng;
+  cudaPointerAttributes pa{};
+  const bool pinned = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();   // an unregistered pointer may leave an error behind
+  std::vector<int> wb(S + 1);
+  for (int s = 0; s <= S; ++s) wb[s] = (int) ((long long) g.n[0] * s / S);
+  cudaEvent_t *ev_in = h->pipe_ev.data(), *ev_dl = h->pipe_ev.data() + S;
+  const AdvanceArgs A = advance_args(h, 0, dt, 0.0);
+  // the primitives of stage v (v = K: the closing c2p's) live in buf(v), the last in the
+  // solver's own PA
+  auto buf = [&](int v) { return (v + K) % 2 == 0 ? h->b.PA : h->pipe_pa; };
+  auto window = [&](int s, int v) {
+    AdvanceArgs W = A;
+    W.g.w0 = wb[s];
+    W.g.w1 = wb[s + 1];
+    W.b.guess = h->pipe_guess;
+    W.b.PA = buf(v);
+    W.b.PAg = v > 0 ? buf(v - 1) : nullptr;
+    return W;
+  };
+  auto phase = [&](const AdvanceArgs &W, int ph, int k) { return fp32(h) ? phase_fp32(W, ph, k) : phase_fp64(W, ph, k); };
+  // the guarded rows [r0, r1) between the host buffer and a device AoS buffer
+  auto copy_rows = [&](double *dst, const double *src, long long r0, long long r1, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+    const size_t off = (size_t) (r0 * s0 * 8);
+    return cudaMemcpyAsync(dst + off, src + off, (size_t) ((r1 - r0) * row_bytes), kind, st);
+  };
+  TransferArgs T = transfer_args(h);
+  T.b.PA = buf(0);
+  TransferArgs Tp = transfer_args(h);
+  Tp.b.PA = buf(K);
+  Tp.pending = 1;
+  auto download_rows = [&](long long r0, long long r1) {
+    return fp32(h) ? download_fp32(Tp, h->pipe_out + r0 * s0 * 8, r0 * s0, (r1 - r0) * s0)
+                   : download_fp64(Tp, h->pipe_out + r0 * s0 * 8, r0 * s0, (r1 - r0) * s0);
+  };
+  // the rows a slab's copy out covers: its own, and for the end slabs the guard rows that
+  // hold their images (slab 0: the right guards, slab S-1: the left guards)
+  auto out_ranges = [&](int s, long long r[3][2]) {
+    int n = 0;
+    r[n][0] = ng + wb[s];
+    r[n][1] = ng + wb[s + 1];
+    ++n;
+    if (s == 0) { r[n][0] = ng + g.n[0]; r[n][1] = G0; ++n; }
+    if (s == S - 1) { r[n][0] = 0; r[n][1] = ng; ++n; }
+    return n;
+  };
+  CK(phase(A, PH_BEGIN, 0));
+  for (const auto &op : pipe_schedule(S, K)) {
+    const int s = op.first, e = op.second;
+    if (e == 0) {
+      // the copy in: the slab's rows, and the end slabs' guard rows (kept for the restore)
+      const long long r0 = s == 0 ? 0 : ng + wb[s], r1 = s == S - 1 ? G0 : ng + wb[s + 1];
+      CK(copy_rows(h->pipe_in, host, r0, r1, cudaMemcpyHostToDevice, h->pipe_h2d));
+      CK(cudaEventRecord(ev_in[s], h->pipe_h2d));
+      CK(cudaStreamWaitEvent(h->stream, ev_in[s], 0));
+      const long long z0 = (ng + wb[s]) * s0, cnt = (long long) (wb[s + 1] - wb[s]) * s0;
+      CK(fp32(h) ? upload_fp32(T, h->pipe_in + z0 * 8, z0, cnt) : upload_fp64(T, h->pipe_in + z0 * 8, z0, cnt));
+    } else if (e == E - 1) {   // download
+      long long r[3][2];
+      const int n = out_ranges(s, r);
+      for (int i = 0; i < n; ++i) CK(download_rows(r[i][0], r[i][1]));
+      if (pinned) {
+        CK(cudaEventRecord(ev_dl[s], h->stream));
+        CK(cudaStreamWaitEvent(h->pipe_d2h, ev_dl[s], 0));
+        for (int i = 0; i < n; ++i)
+          CK(copy_rows(host, h->pipe_out, r[i][0], r[i][1], cudaMemcpyDeviceToHost, h->pipe_d2h));
+      }
+    } else if (e % 2 == 1) {
+      CK(phase(window(s, (e - 1) / 2), PH_FLUX_UPDATE, (e - 1) / 2));
+    } else {
+      CK(phase(window(s, e / 2), PH_C2P, e / 2));
+    }
+  }
+  CK(phase(A, PH_COMMIT, 0));
+  CK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(h->pipe_d2h));
+  CK(cudaStreamSynchronize(h->pipe_h2d));
+  if (h->ctl_host->tc_fault) return fail(h, MGPU_ERR_CUDA, "a tensor-core wait of the learned c2p timed out");
+  const int err = errors_of(*h->ctl_host, h->cfg.rk);
+  if (pinned && err) {          // the copies out went ahead: put the caller's buffer back
+    CK(cudaMemcpyAsync(host, h->pipe_in, (size_t) g.nz * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  } else if (!pinned && !err) {
+    CK(cudaMemcpyAsync(host, h->pipe_out, (size_t) g.nz * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  *errors = err;
+  return MGPU_OK;
+}
+
+int mgpu_set_pipeline(mgpu_solver *h, int slabs)
+{
+  if (!h || slabs < -1 || slabs == 1 || slabs == 2) return fail(h, MGPU_ERR_ARG, "pipeline slabs: 0, -1 or >= 3");
+  h->pipe_slabs = slabs;
+  return MGPU_OK;
+}
+
+int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs)
+{
+  if (!h) return MGPU_ERR_ARG;
+  if (slabs) *slabs = h->pipe_slabs;
+  if (last_slabs) *last_slabs = h->pipe_last;
+  return MGPU_OK;
+}
+
+int mgpu_pipeline_schedule(int slabs, int stages, int *out, int capacity)
+{
+  if (slabs < 3 || stages < 1 || stages > 3 || capacity < 0) return -MGPU_ERR_ARG;
+  const auto sched = pipe_schedule(slabs, stages);
+  if (out) {
+    if (capacity < (int) sched.size()) return -MGPU_ERR_ARG;
+    for (size_t i = 0; i < sched.size(); ++i) {
+      out[2 * i] = sched[i].first;
+      out[2 * i + 1] = sched[i].second;
+    }
+  }
+  return (int) sched.size();
+}
+
 int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors)
 {
   int rc = ensure_ready(h);
   if (rc) return rc;
+  if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
   const auto t0 = std::chrono::steady_clock::now();
-  rc = mgpu_upload_prim(h, host_aos);
-  if (rc) return rc;
   int err = 0;
-  rc = mgpu_advance(h, dt, &err);
-  if (rc) return rc;
-  if (err == 0) {
-    rc = mgpu_download_prim(h, host_aos);
+  const int S = pipe_slab_count(h);
+  h->pipe_last = 0;
+  if (S && pipe_setup(h, S) == 0) {
+    h->pipe_last = S;
+    rc = pipe_advance_host(h, host_aos, dt, S, &err);
     if (rc) return rc;
+  } else {
+    rc = mgpu_upload_prim(h, host_aos);
+    if (rc) return rc;
+    rc = mgpu_advance(h, dt, &err);
+    if (rc) return rc;
+    if (err == 0) {
+      rc = mgpu_download_prim(h, host_aos);
+      if (rc) return rc;
+    }
   }
   const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (kzps) *kzps = 1e-3 * (double) h->g.nz / sec;

@@ -115,7 +115,7 @@ inline cudaError_t launch_diffuse(const AdvanceArgs &A, double r)
   else if (g.nd == 2) k_diffuse_update<T, 2><<<ug, zb, 0, st>>>(g, Un, F, G, H, U1);
   else k_diffuse_update<T, 3><<<ug, zb, 0, st>>>(g, Un, F, G, H, U1);
   k_cons_to_prim<T, 2><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
-      g, StateCPtr<T>{U1.bulk, U1.B}, (T *) b.PA, P0, P1, A.pp, A.ctl, 0, 0, C2P_DIFFUSE, A.ereset, A.preset,
+      g, StateCPtr<T>{U1.bulk, U1.B}, (T *) b.PA, (const T *) b.PA, P0, P1, A.pp, A.ctl, 0, 0, C2P_DIFFUSE, A.ereset, A.preset,
       A.dreset);
   return cudaGetLastError();
 }

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) k_ens_c2p(const BoxDev *boxes, const int2
     for (int s = threadIdx.x; s < tile; s += blockDim.x) {
       const long long t = base + s;
       if (t < d.g.ninterior)
-        c2p_zone<T>(d.g, U, (T *) d.b.PA, Pn, pp, d.ctl, stage, zero_guess, final, ereset, preset, dreset, t);
+        c2p_zone<T>(d.g, U, (T *) d.b.PA, (const T *) d.b.PA, Pn, pp, d.ctl, stage, zero_guess, final, ereset, preset, dreset, t);
     }
   }
 }

@@ -19,25 +19,26 @@
 #endif
 
 namespace mgpu {
-// The learned c2p: the split network + polish kernels with the guesses in `scratch` (a face
-// array, idle while the c2p runs), or the fused kernel.
+// The learned c2p over the grid's window: the split network + polish kernels with the guesses
+// in `scratch` (a face array, idle while a whole-domain c2p runs, or an array of its own, one
+// float2 per interior zone), or the fused kernel.
 template <class T>
-inline void launch_learned_c2p(const Grid &g, cudaStream_t st, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
+inline void launch_learned_c2p(const Grid &g, cudaStream_t st, StateCPtr<T> U, T *PA, const T *PAg, StatePtr<T> Pn0,
                                StatePtr<T> Pn1, const PhysParams &pp, Ctl *ctl, int s, int zero_guess, int mode,
                                int ereset, double preset, double dreset, void *scratch)
 {
-  const long long ntiles = (g.ninterior + 127) / 128;
+  const long long ntiles = (win_tend(g) - win_tbeg(g) + 127) / 128;
   if (MGPU_TC_SPLIT) {
     const long long nmax = 148ll * MGPU_TCNET_CTAS_PER_SM;
     float2 *guess = (float2 *) scratch;
     k_c2p_guess_tc<T><<<(unsigned) (ntiles < nmax ? ntiles : nmax), 128, tc::SMEM_BYTES, st>>>(g, U, Pn0, Pn1, pp,
                                                                                                ctl, s, mode, guess);
-    k_cons_to_prim_guessed<T><<<(unsigned) ntiles, 128, 0, st>>>(g, U, PA, Pn0, Pn1, pp, ctl, s, zero_guess, mode,
+    k_cons_to_prim_guessed<T><<<(unsigned) ntiles, 128, 0, st>>>(g, U, PA, PAg, Pn0, Pn1, pp, ctl, s, zero_guess, mode,
                                                                ereset, preset, dreset, guess);
   } else {
     const long long tmax = 148ll * MGPU_TC_CTAS_PER_SM;
     k_cons_to_prim_tc<T><<<(unsigned) (ntiles < tmax ? ntiles : tmax), 128, tc::SMEM_BYTES, st>>>(
-        g, U, PA, Pn0, Pn1, pp, ctl, s, zero_guess, mode, ereset, preset, dreset);
+        g, U, PA, PAg, Pn0, Pn1, pp, ctl, s, zero_guess, mode, ereset, preset, dreset);
   }
 }
 }  // namespace mgpu
@@ -60,14 +61,6 @@ inline void launch_flux(const Grid &g, int d, int rs, unsigned grid, unsigned bl
 #undef MGPU_FLUX_CASE
 }
 
-// Phases of an advance.  The whole advance is PH_BEGIN, then (PH_C2P, PH_FLUX_UPDATE) per RK
-// stage, then PH_C2P with stage = number of stages (the closing c2p into the uncommitted
-// buffer), then PH_COMMIT.  A decomposed domain exchanges the guard layers of the stage
-// primitives between PH_C2P and PH_FLUX_UPDATE, and sums the error counters over ranks
-// before PH_COMMIT.
-// PH_C2P_SHELL and PH_C2P_CORE together are PH_C2P of a stage (s < number of stages), split
-// so that a decomposed domain can exchange the shell's slabs while the core converts.
-enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3, PH_C2P_SHELL = 4, PH_C2P_CORE = 5 };
 
 // The phases of an advance in the lean layout (rmhd_lean.cuh): no P->U (the committed state
 // is conserved), no c2p at the first stage, sweeps that accumulate into U[!cur], CT from the
@@ -80,19 +73,22 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
   cudaStream_t st = A.stream;
   const StatePtr<T> UA{(T *) b.U0_bulk, b.U0_B}, UB{(T *) b.U1_bulk, b.U1_B};
   T *PA = (T *) b.PA;
+  const T *PAg = b.PAg ? (const T *) b.PAg : PA;   // the stage c2p's previous primitives
   T *Bf = (T *) b.Bf;
   const int ns = num_stages(A.rk);
   LaunchProfiler *pr = A.prof;
-  const unsigned cgrid = (unsigned) ((g.ninterior + 127) / 128);
+  // zone launches cover the grid's window of x rows (the whole interior by default)
+  const long long nwin = win_tend(g) - win_tbeg(g);
+  const unsigned cgrid = (unsigned) ((nwin + 127) / 128);
   const StateCPtr<T> none{nullptr, nullptr};
   auto c2p = [&](int mode, int zero_guess, bool learned) {
-    ProfScope ps(pr, st, KC_C2P, g.ninterior);
+    ProfScope ps(pr, st, KC_C2P, nwin);
     if (learned) {
-      launch_learned_c2p<T>(g, st, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset, A.preset,
-                            A.dreset, b.Bf);
+      launch_learned_c2p<T>(g, st, none, PA, PAg, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset, A.preset,
+                            A.dreset, b.guess ? b.guess : b.Bf);
     } else {
-      k_cons_to_prim<T, 2><<<cgrid, 128, 0, st>>>(g, none, PA, UA, UB, A.pp, A.ctl, s, zero_guess, mode, A.ereset,
-                                                   A.preset, A.dreset);
+      k_cons_to_prim<T, 2><<<cgrid, 128, 0, st>>>(g, none, PA, PAg, UA, UB, A.pp, A.ctl, s, zero_guess, mode,
+                                                   A.ereset, A.preset, A.dreset);
     }
   };
   const bool learned = A.pp.learned && A.pp.mlp_tc;
@@ -115,10 +111,10 @@ inline cudaError_t launch_lean_phase(const AdvanceArgs &A, int phase, int s)
     const StageKind kind = stage_kind(A.rk, s);
     const LeanCombine c = lean_combine(kind.combine);
     for (int d = 1; d <= 3; ++d) {
-      ProfScope ps(pr, st, KC_FLUX, g.ninterior);
+      ProfScope ps(pr, st, KC_FLUX, nwin);
       launch_lean_sweep<T>(g, d, A.pp.riemann, st, PA, UA, UB, Bf, c, A.pp, A.ctl, s);
     }
-    ProfScope ps(pr, st, KC_UPDATE, g.ninterior);
+    ProfScope ps(pr, st, KC_UPDATE, nwin);
     const unsigned zb = 256;
     k_lean_ct<T><<<(unsigned) ((lean_ct_threads(g) + zb - 1) / zb), zb, 0, st>>>(
         g, kind.combine, UA, UB, Bf, A.ctl, s, make_double3(1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz));
@@ -185,14 +181,14 @@ inline cudaError_t launch_phase(const AdvanceArgs &A, int phase, int s)
     const bool simt_net = A.pp.learned && A.pp.mlp && !A.pp.mlp_tc;   // per-thread network guess
     ProfScope ps(pr, st, KC_C2P, g.ninterior);
     if (tc_c2p)
-      launch_learned_c2p<T>(g, st, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset,
+      launch_learned_c2p<T>(g, st, Uin, PA, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset,
                             A.dreset, b.F[0]);
     else if (simt_net)
       k_cons_to_prim<T, 0><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
-          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
+          g, Uin, PA, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
     else
       k_cons_to_prim<T, 2><<<(unsigned) ((g.ninterior + 127) / 128), 128, 0, st>>>(
-          g, Uin, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
+          g, Uin, PA, PA, Pc0, Pc1, A.pp, A.ctl, s, zero_guess, final, A.ereset, A.preset, A.dreset);
   } else if (phase == PH_FLUX_UPDATE) {
     if (A.godunov)
       launch_ctu_stage<T>(A, s, s == 0 ? StateCPtr<T>{U0.bulk, U0.B} : StateCPtr<T>{U1.bulk, U1.B});
@@ -319,7 +315,8 @@ inline cudaError_t launch_download(const TransferArgs &A, double *d_aos, long lo
   if (A.lean) {
     k_lean_download<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count, (const T *) A.b.PA,
                                                    StateCPtr<T>{(const T *) A.b.U0_bulk, A.b.U0_B},
-                                                   StateCPtr<T>{(const T *) A.b.U1_bulk, A.b.U1_B}, A.ctl);
+                                                   StateCPtr<T>{(const T *) A.b.U1_bulk, A.b.U1_B}, A.ctl,
+                                                   A.pending);
     return cudaGetLastError();
   }
   k_state_to_aos<T><<<grid, blk, 0, A.stream>>>(A.g, d_aos, z0, count,

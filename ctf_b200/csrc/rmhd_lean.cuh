@@ -98,9 +98,13 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
   lean_regs(ctl, UA, UB, U0, U1);
   const int d = dim - 1;
   const int oa = dim == 1 ? 1 : 0;                  // the other two dimensions: a (outer), k (inner)
-  const int na = g.n[oa] + 2, nk = g.n[2] + 2;
+  // the window of x rows: the x sweep marches over its rows, the y sweep takes its columns
+  // (with one halo row each side)
+  const int alo = dim == 2 ? win_lo(g) : 0, ahi = dim == 2 ? win_hi(g) : g.n[oa];
+  const int mlo = dim == 1 ? win_lo(g) : 0, mhi = dim == 1 ? win_hi(g) : g.n[d];
+  const int na = ahi - alo + 2, nk = g.n[2] + 2;
   const long long ncol = (long long) na * nk;
-  const int nchunk = (g.n[d] + chunk_len - 1) / chunk_len;
+  const int nchunk = (mhi - mlo + chunk_len - 1) / chunk_len;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
@@ -109,13 +113,14 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
   if (t < ncol * nchunk) {
     const int chunk = (int) (t / ncol);
     const long long col = t - (long long) chunk * ncol;
-    const int a = (int) (col / nk), b = (int) (col - (long long) a * nk);
+    const int ar = (int) (col / nk), b = (int) (col - (long long) ar * nk);
+    const int a = alo + ar;
     const int ca = g.ng - 1 + a, k = g.ng - 1 + b;
-    const bool interior = a >= 1 && a <= g.n[oa] && b >= 1 && b <= g.n[2];
+    const bool interior = a >= alo + 1 && a <= ahi && b >= 1 && b <= g.n[2];
     const long long S = g.s[d];
     const long long base = (long long) ca * g.s[oa] + k;   // zone (0 along dim, ca, k)
-    const int m0 = g.ng + chunk * chunk_len;
-    const int m1 = min(m0 + chunk_len, g.ng + g.n[d]);
+    const int m0 = g.ng + mlo + chunk * chunk_len;
+    const int m1 = min(m0 + chunk_len, g.ng + mhi);
     const T inv_dx = T(1.0 / (dim == 1 ? g.dx : g.dy));
     const T dt = T(ctl->dt);
     T *slot0 = Bf + (long long) bf_slot(dim, dim == 1 ? By : Bx) * g.cs;
@@ -159,7 +164,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
   StatePtr<T> U0, U1;
   lean_regs(ctl, UA, UB, U0, U1);
   const int nf = g.n[2] + 1, nj = g.n[1] + 2;
-  const long long total = (long long) (g.n[0] + 2) * nj * nf;
+  const int alo = win_lo(g), ahi = win_hi(g);   // the window's x rows, one halo row each side
+  const long long total = (long long) (ahi - alo + 2) * nj * nf;
   const long long q = (long long) blockIdx.x * 127 - 1 + threadIdx.x;
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
@@ -171,7 +177,8 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
   if (active) {
     const long long row = q / nf;
     const int fk = (int) (q - row * nf);              // face fk + ng - 1
-    const int a = (int) (row / nj), b = (int) (row - (long long) a * nj);
+    const int ar = (int) (row / nj), b = (int) (row - (long long) ar * nj);
+    const int a = alo + ar;
     const int i = g.ng - 1 + a, j = g.ng - 1 + b;
     f = (long long) i * g.s[0] + (long long) j * g.s[1] + (g.ng - 1 + fk);
 #pragma unroll
@@ -185,7 +192,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
     }
 #pragma unroll
     for (int r = 0; r < 5; ++r) fs[r][threadIdx.x] = Fo[r];
-    upd = threadIdx.x > 0 && fk >= 1 && a >= 1 && a <= g.n[0] && b >= 1 && b <= g.n[1];
+    upd = threadIdx.x > 0 && fk >= 1 && a >= alo + 1 && a <= ahi && b >= 1 && b <= g.n[1];
   }
   __syncthreads();
   if (upd) {
@@ -252,12 +259,12 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int c
   if (stage_failed(ctl, stage + 1)) return;
   const long long npair = (g.n[2] + 1) / 2;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long) g.n[0] * g.n[1] * npair) return;
+  if (t >= (long long) win_rows(g) * g.n[1] * npair) return;
   StatePtr<T> U0, U1;
   lean_regs(ctl, UA, UB, U0, U1);
   const int kp = (int) (t % npair);
   const long long ij = t / npair;
-  const int j = (int) (ij % g.n[1]), i = (int) (ij / g.n[1]);
+  const int j = (int) (ij % g.n[1]), i = win_lo(g) + (int) (ij / g.n[1]);
   const int k = 2 * kp;
   const long long z = ((long long) (i + g.ng) * g.G[1] + (j + g.ng)) * g.G[2] + (k + g.ng);
   const double dtd = ctl->dt;
@@ -265,8 +272,8 @@ __global__ void __launch_bounds__(256, MGPU_UPDATE_MINB) k_lean_ct(Grid g, int c
   if (k + 1 < g.n[2]) lean_ct_zone<T>(g, combine, U0, U1, Bf, dtd, inv, z + 1);
 }
 
-// Threads of k_lean_ct for a grid (two zones along k each).
-inline long long lean_ct_threads(const Grid &g) { return (long long) g.n[0] * g.n[1] * ((g.n[2] + 1) / 2); }
+// Threads of k_lean_ct for a grid's window (two zones along k each).
+inline long long lean_ct_threads(const Grid &g) { return (long long) win_rows(g) * g.n[1] * ((g.n[2] + 1) / 2); }
 
 // ---- commit of the lean layout ------------------------------------------------------------------
 // As k_commit, then the restore c2p (C2P_LEAN_RESTORE) runs when nothing was committed.
@@ -310,15 +317,17 @@ __global__ void k_lean_upload(Grid g, const double *__restrict__ aos, long long 
       }
 }
 
-// Download: the committed primitives are PA's bulk components and U[cur]'s field.
+// Download: the committed primitives are PA's bulk components and U[cur]'s field.  pending = 1
+// reads an advance's result before its commit: after the closing c2p, PA's bulk components and
+// the field of the register U[!cur].
 template <class T>
 __global__ void k_lean_download(Grid g, double *__restrict__ aos, long long z0, long long count, const T *PA,
-                                StateCPtr<T> UA, StateCPtr<T> UB, const Ctl *ctl)
+                                StateCPtr<T> UA, StateCPtr<T> UB, const Ctl *ctl, int pending)
 {
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const long long z = z0 + t;
-  const StateCPtr<T> U = ctl->cur ? UB : UA;
+  const StateCPtr<T> U = (ctl->cur ^ pending) ? UB : UA;
 #pragma unroll
   for (int q = 0; q < 5; ++q) aos[t * 8 + q] = double(PA[q * g.cs + z]);
 #pragma unroll
@@ -353,7 +362,7 @@ inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, c
 {
   const unsigned blk = 128;
   if (dim == 3) {
-    const long long total = (long long) (g.n[0] + 2) * (g.n[1] + 2) * (g.n[2] + 1);
+    const long long total = (long long) (win_rows(g) + 2) * (g.n[1] + 2) * (g.n[2] + 1);
     const unsigned grid = (unsigned) ((total + 126) / 127);
 #define MGPU_LEANZ_CASE(R) \
   if (rs == R) { k_lean_sweep_z<T, R><<<grid, blk, 0, st>>>(g, PA, UA, UB, Bf, c, pp, ctl, s); return; }
@@ -361,10 +370,13 @@ inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, c
 #undef MGPU_LEANZ_CASE
     return;
   }
-  const int oa = dim == 1 ? 1 : 0;
-  const long long ncol = (long long) (g.n[oa] + 2) * (g.n[2] + 2);
-  const int L = lean_chunk(ncol, g.n[dim - 1], 148ll * MGPU_FLUX_MINB * blk);
-  const long long nchunk = (g.n[dim - 1] + L - 1) / L;
+  // x sweep: columns over (y, z), marching over the window's rows; y sweep: columns over the
+  // window's rows (one halo row each side) and z, marching over y
+  const long long ncol = dim == 1 ? (long long) (g.n[1] + 2) * (g.n[2] + 2)
+                                  : (long long) (win_rows(g) + 2) * (g.n[2] + 2);
+  const int nmarch = dim == 1 ? win_rows(g) : g.n[1];
+  const int L = lean_chunk(ncol, nmarch, 148ll * MGPU_FLUX_MINB * blk);
+  const long long nchunk = (nmarch + L - 1) / L;
   const unsigned grid = (unsigned) ((ncol * nchunk + blk - 1) / blk);
 #define MGPU_LEAN_CASE(D, R) \
   if (dim == D && rs == R) { k_lean_sweep<T, D, R><<<grid, blk, 0, st>>>(g, PA, UA, UB, Bf, c, pp, ctl, s, L); return; }

@@ -246,9 +246,11 @@ __device__ __forceinline__ bool c2p_skip(const Ctl *ctl, int stage, int final)
 
 // One interior zone's c2p.  Guess: 0 compiles in the per-thread network guess (used when
 // pp.learned), 2 leaves it out -- the network's activations would otherwise set the register
-// and stack budget of every c2p launch.
+// and stack budget of every c2p launch.  PAg holds the previous primitives the ladder may start
+// from (PA itself, except in the pipelined host advance, whose stages alternate two arrays).
 template <class T, int Guess = 2>
-__device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, StatePtr<T> Pn, const PhysParams &pp,
+__device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, const T *PAg, StatePtr<T> Pn,
+                                         const PhysParams &pp,
                                          Ctl *ctl, int stage, int zero_guess, int final, int ereset, double preset,
                                          double dreset, long long t)
 {
@@ -260,7 +262,7 @@ __device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, S
   // the previous primitives are read only when the ladder needs them or a failure keeps them
   const auto prev = [&](double *q) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+    for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PAg[c * g.cs + z]);
   };
   C2PTally tally;
   const int err = cons_to_prim<(sizeof(T) < sizeof(double)), Guess>(pp, u, p, &tally, 0.0, 0.0, true, prev) != 0;
@@ -268,16 +270,17 @@ __device__ __forceinline__ void c2p_zone(const Grid &g, StateCPtr<T> U, T *PA, S
 }
 
 template <class T, int Guess>
-__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0, StatePtr<T> Pn1,
+__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim(Grid g, StateCPtr<T> U, T *PA, const T *PAg,
+                                                      StatePtr<T> Pn0, StatePtr<T> Pn1,
                                                       PhysParams pp, Ctl *ctl, int stage, int zero_guess, int final,
                                                       int ereset, double preset, double dreset)
 {
   if (c2p_skip(ctl, stage, final)) return;
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
+  const long long t = win_tbeg(g) + (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= win_tend(g)) return;
   // the uncommitted buffer, or for Mara.diffuse the committed one (rewritten in place)
   const int target = final == C2P_DIFFUSE ? ctl->cur : ctl->cur ^ 1;
-  c2p_zone<T, Guess>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess,
+  c2p_zone<T, Guess>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, PAg, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess,
                      final, ereset, preset, dreset, t);
 }
 
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_region(Grid
   interior_coords(g, t, i, j, k);
   if (in_shell(g, i, j, k) != (region == 1)) return;
   const int target = ctl->cur ^ 1;
-  c2p_zone<T, 2>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess, final,
+  c2p_zone<T, 2>(g, c2p_input(ctl, final, U, Pn0, Pn1), PA, PA, target ? Pn1 : Pn0, pp, ctl, stage, zero_guess, final,
                  ereset, preset, dreset, t);
 }
 

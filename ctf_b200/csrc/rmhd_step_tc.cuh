@@ -17,7 +17,7 @@ namespace mgpu {
 #endif
 
 template <class T>
-__global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Grid g, StateCPtr<T> U, T *PA, StatePtr<T> Pn0,
+__global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Grid g, StateCPtr<T> U, T *PA, const T *PAg, StatePtr<T> Pn0,
                                                          StatePtr<T> Pn1, PhysParams pp, Ctl *ctl, int stage,
                                                          int zero_guess, int final, int ereset, double preset,
                                                          double dreset)
@@ -26,10 +26,11 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
   extern __shared__ unsigned char tc_smem[];
   tc::TcNet net = tc::tc_setup(tc_smem, (const unsigned char *) pp.mlp_tc);
   U = c2p_input(ctl, final, U, Pn0, Pn1);
-  const long long ntiles = (g.ninterior + 127) / 128;
+  const long long tb = win_tbeg(g), te = win_tend(g);
+  const long long ntiles = (te - tb + 127) / 128;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long t = tile * 128 + threadIdx.x;
-    const bool valid = t < g.ninterior;
+    const long long t = tb + tile * 128 + threadIdx.x;
+    const bool valid = t < te;
     int i = 0, j = 0, k = 0;
     long long z = 0;
     double u[8], p[8];
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(128, MGPU_TC_CTAS_PER_SM) k_cons_to_prim_tc(Gr
     // the previous primitives are read only when the ladder needs them or a failure keeps them
     const auto prev = [&](double *q) {
 #pragma unroll
-      for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+      for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PAg[c * g.cs + z]);
     };
     const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use, prev) != 0;
     c2p_finish<T>(g, PA, ctl->cur ? Pn0 : Pn1, ctl, stage, final, ereset, preset, dreset, i, j, k, u, p, err,
@@ -87,10 +88,11 @@ __global__ void __launch_bounds__(128, MGPU_TCNET_CTAS_PER_SM) k_c2p_guess_tc(Gr
   extern __shared__ unsigned char tc_smem[];
   tc::TcNet net = tc::tc_setup(tc_smem, (const unsigned char *) pp.mlp_tc);
   U = c2p_input(ctl, final, U, Pn0, Pn1);
-  const long long ntiles = (g.ninterior + 127) / 128;
+  const long long tb = win_tbeg(g), te = win_tend(g);
+  const long long ntiles = (te - tb + 127) / 128;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long t = tile * 128 + threadIdx.x;
-    const bool valid = t < g.ninterior;
+    const long long t = tb + tile * 128 + threadIdx.x;
+    const bool valid = t < te;
     float xn[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     bool good = false;
     if (valid) {
@@ -119,7 +121,7 @@ __global__ void __launch_bounds__(128, MGPU_TCNET_CTAS_PER_SM) k_c2p_guess_tc(Gr
 }
 
 template <class T>
-__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_guessed(Grid g, StateCPtr<T> U, T *PA,
+__global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_guessed(Grid g, StateCPtr<T> U, T *PA, const T *PAg,
                                                                            StatePtr<T> Pn0, StatePtr<T> Pn1,
                                                                            PhysParams pp, Ctl *ctl, int stage,
                                                                            int zero_guess, int final, int ereset,
@@ -127,8 +129,8 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_guessed(Gri
                                                                            const float2 *guess)
 {
   if (c2p_skip(ctl, stage, final)) return;
-  const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.ninterior) return;
+  const long long t = win_tbeg(g) + (long long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= win_tend(g)) return;
   const StateCPtr<T> Uz = c2p_input(ctl, final, U, Pn0, Pn1);
   int i, j, k;
   interior_coords(g, t, i, j, k);
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(128, MGPU_C2P_MINB) k_cons_to_prim_guessed(Gri
   // the previous primitives are read only when the ladder needs them or a failure keeps them
   const auto prev = [&](double *q) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PA[c * g.cs + z]);
+    for (int c = 0; c < 8; ++c) q[c] = zero_guess ? 0.0 : double(PAg[c * g.cs + z]);
   };
   C2PTally tally;
   const int err = cons_to_prim<(sizeof(T) < sizeof(double)), 1>(pp, u, p, &tally, Zg, Wg, use, prev) != 0;

@@ -120,7 +120,19 @@ struct Grid {
   // guarded arrays, over all ranks, that hold interior index m of d (device, n[d] entries).
   int ext[3];
   const int *mult[3];
+  // Window of the lean-layout launches: interior x rows [w0, w1) (w1 == 0: all rows).  A
+  // window's launches read the rows within the stencil's reach around it and write only its
+  // own rows (plus one halo row each side of the face fields, with the values the
+  // neighbouring window writes there too).
+  int w0, w1;
 };
+
+__host__ __device__ inline int win_lo(const Grid &g) { return g.w1 ? g.w0 : 0; }
+__host__ __device__ inline int win_hi(const Grid &g) { return g.w1 ? g.w1 : g.n[0]; }
+__host__ __device__ inline int win_rows(const Grid &g) { return win_hi(g) - win_lo(g); }
+// The window's interior flat indices: [win_tbeg, win_tend)
+__host__ __device__ inline long long win_tbeg(const Grid &g) { return (long long) win_lo(g) * g.n[1] * g.n[2]; }
+__host__ __device__ inline long long win_tend(const Grid &g) { return (long long) win_hi(g) * g.n[1] * g.n[2]; }
 
 template <class T> struct StatePtr {   // components 0..4 in T, 5..7 in double
   T *bulk;
@@ -180,6 +192,8 @@ struct AdvanceBuffers {
   void *F[3];
   void *Pd[3];   // CTU-Hancock: predicted primitives per direction (8 x T each)
   void *Bf;      // lean layout: the six transverse magnetic face fluxes (6 x T)
+  void *guess;   // learned c2p guesses, one float2 per interior zone (nullptr: Bf is the scratch)
+  void *PAg;     // lean stage c2p: the previous primitives the ladder may start from (nullptr: PA)
 };
 
 // Optional per-launch timing: the launcher records an event pair around every kernel and
@@ -212,6 +226,15 @@ struct ProfScope {
     if (slot >= 0) cudaEventRecord(p->ev[2 * slot + 1], s);
   }
 };
+
+// Phases of an advance.  The whole advance is PH_BEGIN, then (PH_C2P, PH_FLUX_UPDATE) per RK
+// stage, then PH_C2P with stage = number of stages (the closing c2p into the uncommitted
+// buffer), then PH_COMMIT.  A decomposed domain exchanges the guard layers of the stage
+// primitives between PH_C2P and PH_FLUX_UPDATE, and sums the error counters over ranks
+// before PH_COMMIT.
+// PH_C2P_SHELL and PH_C2P_CORE together are PH_C2P of a stage (s < number of stages), split
+// so that a decomposed domain can exchange the shell's slabs while the core converts.
+enum Phase { PH_BEGIN = 0, PH_C2P = 1, PH_FLUX_UPDATE = 2, PH_COMMIT = 3, PH_C2P_SHELL = 4, PH_C2P_CORE = 5 };
 
 struct AdvanceArgs {
   Grid g;
@@ -263,6 +286,7 @@ struct TransferArgs {
   int cur;   // committed buffer, for the halo copies of the committed state
   int lean = 0;        // lean layout: the committed state is (PA, U[cur]); see rmhd_lean.cuh
   double gamma = 0.0;  // for the lean upload's P->U
+  int pending = 0;     // lean download of an advance's result before its commit (k_lean_download)
 };
 
 // One member of an ensemble of boxes (device-side descriptor).

@@ -43,6 +43,15 @@ struct mgpu_solver {
   int prof_count = 0;
   mgpu::LaunchProfiler prof{};
   bool prof_on = false;
+  // pipelined mgpu_advance_host (lean layout): device copies of the AoS buffer in and out, a
+  // second stage-primitive array, the learned c2p's guesses, copy streams and per-slab events
+  int pipe_slabs = -1;          // 0 off, -1 automatic, else the slab count
+  int pipe_last = 0;            // slabs of the last mgpu_advance_host (0: unpipelined)
+  int pipe_state = 0;           // 0 not set up, 1 ready, -1 not enough device memory
+  double *pipe_in = nullptr, *pipe_out = nullptr;
+  void *pipe_guess = nullptr, *pipe_pa = nullptr;
+  cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
+  std::vector<cudaEvent_t> pipe_ev;
 };
 
 

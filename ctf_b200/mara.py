@@ -176,6 +176,16 @@ class Solver:
                                                ctypes.byref(e)))
         return kz.value, e.value
 
+    def set_pipeline(self, slabs: int):
+        """Slabs of the pipelined advance_host: 0 off, -1 automatic (the default), >= 3."""
+        self._check(self.lib.mgpu_set_pipeline(self.h, int(slabs)))
+
+    def pipeline(self) -> tuple[int, int]:
+        """(the slab setting, the slabs the last advance_host used -- 0 when unpipelined)."""
+        s, last = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.mgpu_get_pipeline(self.h, ctypes.byref(s), ctypes.byref(last)))
+        return s.value, last.value
+
     def advance_async(self, n: int, dt: float | None = None, cfl: float = 0.3):
         mode = 0 if dt is not None else 1
         self._check(self.lib.mgpu_advance_async(self.h, int(n), mode, ctypes.c_double(dt or 0.0),

@@ -127,8 +127,22 @@ int mgpu_download_prim_range(mgpu_solver *h, double *host_aos, long long z0, lon
  * returns in *errors the number of failed zones (state unchanged when > 0).  Synchronous. */
 int mgpu_advance(mgpu_solver *h, double dt, int *errors);
 /* Mara.advance(buf, dt) exactly: copies the host buffer in, advances, copies it back when
- * errors == 0; *kzps is 1e-3 * zones (guards included) / wall seconds of the call. */
+ * errors == 0; *kzps is 1e-3 * zones (guards included) / wall seconds of the call.
+ * In the 3-D lean layout the call is pipelined over slabs of x rows when device memory allows
+ * (two device copies of the AoS buffer and a second stage-primitive array): the copy in, the
+ * advance's stages and the copy out of different slabs overlap.  The result is the same as the unpipelined call's, bit for bit, and
+ * when the advance fails the buffer gets its original contents back. */
 int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors);
+/* Slab count of the pipelined mgpu_advance_host: 0 off, -1 automatic (the default: about 11
+ * rows per slab), >= 3 that many (at least 4 x rows each).  *last_slabs (may be NULL) gets the
+ * count the previous mgpu_advance_host used, 0 when it ran unpipelined. */
+int mgpu_set_pipeline(mgpu_solver *h, int slabs);
+int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs);
+/* The pipelined advance's issue order for `slabs` slabs and `stages` Runge-Kutta stages, as
+ * (slab, operation) pairs into out[2*i], out[2*i+1] (operation 0 the upload, 2k+1 stage k's
+ * sweeps and CT, 2k stage k's c2p -- 2*stages the closing one -- and 2*stages+1 the download).
+ * Returns the number of pairs (out may be NULL), or -MGPU_ERR_ARG.  Needs no GPU. */
+int mgpu_pipeline_schedule(int slabs, int stages, int *out, int capacity);
 /* Enqueue n advances without host synchronisation: dt_mode 0 uses `dt` for every step,
  * dt_mode 1 takes each step's dt = cfl*min_dx/MaxLambda of the step before (the first step
  * uses the MaxLambda left by the previous advance).  A step that fails is not committed;

@@ -1,0 +1,105 @@
+"""The issue order of the pipelined host advance (mgpu_pipeline_schedule), checked on the CPU
+against a model of what each operation reads and writes.
+
+The model tracks, per interior x row, which stage's primitives each of the two stage arrays
+holds (stage v lives in array (v + K) % 2, so the closing c2p's in the solver's own) and which
+stage's sum the Runge-Kutta register holds.  Each operation asserts that every row it reads
+holds the version it needs -- not yet written (a read before the producer) and already
+overwritten (a write before the last reader) both fail -- and then writes its own rows.
+Rows are periodic in x (the end slabs' guard images are their neighbours' rows).  A sweep
+reads the stage primitives up to three rows beyond its slab (WENO5); the face fields CT reads
+one row beyond the slab are written by the same operation's sweeps, so they need no check.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from ctf_b200 import _lib
+
+REACH = 3   # rows of stage primitives a sweep reads beyond its slab
+
+
+def schedule(S, K):
+    lib = _lib.load()
+    n = lib.mgpu_pipeline_schedule(S, K, None, 0)
+    assert n > 0
+    out = (ctypes.c_int * (2 * n))()
+    assert lib.mgpu_pipeline_schedule(S, K, out, 2 * n) == n
+    return [(out[2 * i], out[2 * i + 1]) for i in range(n)]
+
+
+def simulate(S, K, n0):
+    """Runs the schedule against the row model; returns the order the slabs finished in."""
+    E = 2 * K + 2
+    wb = [n0 * s // S for s in range(S + 1)]
+    pa = np.full((2, n0), -1)  # stage of the primitives in each stage array (-1: none yet)
+    reg = np.full(n0, -1)      # last stage whose sweeps were added into the register
+    finished = []
+
+    def rows(s, ext=0):
+        return np.arange(wb[s] - ext, wb[s + 1] + ext) % n0
+
+    def arr(v):
+        return pa[(v + K) % 2]
+
+    for s, e in schedule(S, K):
+        own = rows(s)
+        if e == 0:                                  # upload: the committed primitives
+            arr(0)[own] = 0
+        elif e == E - 1:                            # download of the result
+            assert (arr(K)[own] == K).all() and (reg[own] == K - 1).all(), (s, e)
+            finished.append(s)
+        elif e % 2 == 1:                            # stage k's sweeps + CT
+            k = (e - 1) // 2
+            assert (arr(k)[rows(s, REACH)] == k).all(), (s, e)
+            assert (reg[own] == k - 1).all(), (s, e)
+            reg[own] = k
+        else:                                       # stage k's c2p (k = K: the closing one)
+            k = e // 2
+            assert (reg[own] == k - 1).all(), (s, e)
+            assert (arr(k - 1)[own] == k - 1).all(), (s, e)  # the previous primitives seed the ladder
+            arr(k)[own] = k
+    assert (arr(K) == K).all() and (reg == K - 1).all()
+    return finished
+
+
+@pytest.mark.parametrize("K", [1, 2, 3])
+@pytest.mark.parametrize("S", [3, 4, 5, 7, 8, 16, 33])
+def test_schedule_respects_every_read(S, K):
+    for n0 in (4 * S, 4 * S + 3, 32 * S):
+        finished = simulate(S, K, n0)
+        assert sorted(finished) == list(range(S))
+
+
+@pytest.mark.parametrize("S,K", [(3, 3), (16, 3), (9, 2)])
+def test_schedule_shape(S, K):
+    """Every operation once, in order per slab; uploads outward from slab 0; the first
+    downloads come before the last uploads when there are enough slabs to overlap them."""
+    sched = schedule(S, K)
+    E = 2 * K + 2
+    assert len(sched) == S * E
+    per = {s: [e for t, e in sched if t == s] for s in range(S)}
+    assert all(per[s] == list(range(E)) for s in range(S))
+    ups = [s for s, e in sched if e == 0]
+    ring = [0] + [x for d in range(1, S) for x in (d, S - d)]
+    assert ups == list(dict.fromkeys(ring))[:S]
+    if S >= 16:
+        first_dl = next(i for i, (s, e) in enumerate(sched) if e == E - 1)
+        last_up = max(i for i, (s, e) in enumerate(sched) if e == 0)
+        assert first_dl < last_up
+
+
+def test_schedule_arguments_are_checked():
+    lib = _lib.load()
+    assert lib.mgpu_pipeline_schedule(2, 3, None, 0) < 0
+    assert lib.mgpu_pipeline_schedule(4, 0, None, 0) < 0
+    assert lib.mgpu_pipeline_schedule(4, 4, None, 0) < 0
+    out = (ctypes.c_int * 4)()
+    assert lib.mgpu_pipeline_schedule(4, 3, out, 4) < 0      # too small for 32 pairs
+
+
+def test_pipeline_setting_needs_a_handle():
+    lib = _lib.load()
+    assert lib.mgpu_set_pipeline(None, -1) == 1
+    assert lib.mgpu_get_pipeline(None, None, None) == 1

@@ -64,6 +64,95 @@ def simulate(S, K, n0):
     return finished
 
 
+def dependencies(S, K, s, e):
+    """The operations that (s, e) waits for: the slab's previous one, and for sweeps (odd e
+    below the download) the neighbours' previous ones."""
+    E = 2 * K + 2
+    if e == 0:
+        return []
+    deps = [(s, e - 1)]
+    if e % 2 == 1 and e != E - 1:
+        deps += [((s - 1) % S, e - 1), ((s + 1) % S, e - 1)]
+    return deps
+
+
+def check_dag(S, K, n0):
+    """Every hazard ordered by the dependency graph alone, not only by the issue order (so the
+    operations could also run on several streams): a read's producer and a write's previous
+    writer and readers are ancestors.  Face fields: a sweep operation writes its own rows and one halo row each side,
+    then CT reads them; two writers of the same stage's face fields write the same values."""
+    E = 2 * K + 2
+    wb = [n0 * s // S for s in range(S + 1)]
+    anc = {}
+    for op in schedule(S, K):
+        a = set()
+        for d in dependencies(S, K, *op):
+            assert d in anc, (op, d)          # issued before its dependencies would deadlock
+            a |= anc[d] | {d}
+        anc[op] = a
+    # per (array, row): [version, writers of that version, readers]
+    state = {}
+
+    def rows(s, ext=0):
+        return [r % n0 for r in range(wb[s] - ext, wb[s + 1] + ext)]
+
+    def done_before(x, op):
+        return x == op or x in anc[op]
+
+    def read(op, arr, rs, version):
+        for r in rs:
+            v, writers, readers = state[(arr, r)]
+            assert v == version, (op, arr, r, v, version)
+            assert any(done_before(w, op) for w in writers), (op, arr, r, writers)
+            readers.add(op)
+
+    def write(op, arr, rs, version, same_value_ok=False):
+        for r in rs:
+            old = state.get((arr, r))
+            if old is not None:
+                v, writers, readers = old
+                if same_value_ok and v == version:            # the same stage's face fields
+                    writers.add(op)
+                    continue
+                assert all(done_before(w, op) for w in writers), (op, arr, r, writers)
+                assert all(done_before(x, op) for x in readers), (op, arr, r)
+            state[(arr, r)] = [version, {op}, set()]
+
+    def pa(v):
+        return "pa%d" % ((v + K) % 2)
+
+    for op in schedule(S, K):
+        s, e = op
+        own = rows(s)
+        if e == 0:
+            write(op, pa(0), own, 0)
+            write(op, "u0", own, 0)
+        elif e == E - 1:
+            read(op, pa(K), own, K)
+            read(op, "u1", own, K - 1)
+        elif e % 2 == 1:
+            k = (e - 1) // 2
+            read(op, pa(k), rows(s, REACH), k)
+            read(op, "u0", own, 0)
+            if k > 0:
+                read(op, "u1", own, k - 1)
+            write(op, "u1", own, k)
+            write(op, "bf", rows(s, 1), k, same_value_ok=True)
+            read(op, "bf", rows(s, 1), k)
+        else:
+            k = e // 2
+            read(op, "u1", own, k - 1)
+            read(op, pa(k - 1), own, k - 1)
+            write(op, pa(k), own, k)
+
+
+@pytest.mark.parametrize("K", [1, 2, 3])
+@pytest.mark.parametrize("S", [3, 4, 5, 7, 8, 16, 33])
+def test_dependencies_order_every_hazard(S, K):
+    for n0 in (4 * S, 4 * S + 3):
+        check_dag(S, K, n0)
+
+
 @pytest.mark.parametrize("K", [1, 2, 3])
 @pytest.mark.parametrize("S", [3, 4, 5, 7, 8, 16, 33])
 def test_schedule_respects_every_read(S, K):

@@ -596,8 +596,10 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
 // (e odd) may run once the operation before them has run on the slab and on both neighbouring
 // slabs (periodic in x: slab 0's images lie next to slab S-1), because they read the
 // neighbours' stage primitives up to three rows deep; a c2p or a download needs only the
-// slab's own previous operation (CT reads face fields one row beyond the slab, which the same
-// operation's sweeps compute).  Each window launch computes exactly the faces and zones of the
+// slab's own previous operation.  CT reads y and z face fields one row beyond the slab: the
+// same operation's sweeps compute those halo rows, except the one next to the neighbour
+// toward slab 0 (pipe_pred), whose sweeps of the same stage computed it as their own row and
+// run first.  Each window launch computes exactly the faces and zones of the
 // whole-box launch that fall in it, so the result is the whole-box advance's.
 // The slabs are uploaded outward from slab 0 in both directions, so that slab 0's neighbourhood
 // arrives first; after each upload the compute stream takes every operation that became ready,
@@ -669,6 +671,24 @@ static int pipe_setup(mgpu_solver *h, int S)
   return 0;
 }
 
+// The neighbour whose sweeps a slab's sweeps wait for, so as to reuse the y and z face fields
+// of the halo row they computed as their own (-1: none, the slab computes both halo rows).  The
+// slabs on either side of slab 0, uploaded outward from it, take the one toward slab 0; slab 0
+// and slab S-1 compute both (their outer halo rows are guard rows no other slab computes).
+static int pipe_pred(int S, int s)
+{
+  if (s >= 1 && s <= S / 2) return s - 1;
+  if (s > S / 2 && s <= S - 2) return s + 1;
+  return -1;
+}
+
+// Grid::whskip of a slab's sweeps: the halo row its pipe_pred neighbour computes.
+static int pipe_whskip(int S, int s)
+{
+  const int p = pipe_pred(S, s);
+  return p < 0 ? 0 : (p == s - 1 ? 1 : 2);
+}
+
 // The order in which the pipelined advance issues its operations: (slab, operation) pairs,
 // the uploads included, for S slabs and K Runge-Kutta stages.
 static std::vector<std::pair<int, int>> pipe_schedule(int S, int K)
@@ -682,7 +702,10 @@ static std::vector<std::pair<int, int>> pipe_schedule(int S, int K)
     if ((int) order.size() < S) order.push_back(S - d);
   }
   auto ready = [&](int s, int e) {
-    return done[s] == e && (e % 2 == 0 || e == E - 1 || (done[(s + S - 1) % S] >= e && done[(s + 1) % S] >= e));
+    if (done[s] != e) return false;
+    if (e % 2 == 0 || e == E - 1) return true;
+    const int p = pipe_pred(S, s);
+    return done[(s + S - 1) % S] >= e && done[(s + 1) % S] >= e && (p < 0 || done[p] > e);
   };
   for (int u : order) {
     out.emplace_back(u, 0);
@@ -725,6 +748,7 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, int S, int
     W.b.guess = h->pipe_guess;
     W.b.PA = buf(v);
     W.b.PAg = v > 0 ? buf(v - 1) : nullptr;
+    W.g.whskip = pipe_whskip(S, s);
     return W;
   };
   auto phase = [&](const AdvanceArgs &W, int ph, int k) { return fp32(h) ? phase_fp32(W, ph, k) : phase_fp64(W, ph, k); };

@@ -99,10 +99,11 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
   const int d = dim - 1;
   const int oa = dim == 1 ? 1 : 0;                  // the other two dimensions: a (outer), k (inner)
   // the window of x rows: the x sweep marches over its rows, the y sweep takes its columns
-  // (with one halo row each side)
+  // (rows a - 1 in [win_flo, win_fhi): its own and the halo rows it computes)
   const int alo = dim == 2 ? win_lo(g) : 0, ahi = dim == 2 ? win_hi(g) : g.n[oa];
+  const int a0 = dim == 2 ? win_flo(g) + 1 : 0, na = dim == 2 ? win_fhi(g) - win_flo(g) : g.n[oa] + 2;
   const int mlo = dim == 1 ? win_lo(g) : 0, mhi = dim == 1 ? win_hi(g) : g.n[d];
-  const int na = ahi - alo + 2, nk = g.n[2] + 2;
+  const int nk = g.n[2] + 2;
   const long long ncol = (long long) na * nk;
   const int nchunk = (mhi - mlo + chunk_len - 1) / chunk_len;
   const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep(Grid g, cons
     const int chunk = (int) (t / ncol);
     const long long col = t - (long long) chunk * ncol;
     const int ar = (int) (col / nk), b = (int) (col - (long long) ar * nk);
-    const int a = alo + ar;
+    const int a = a0 + ar;
     const int ca = g.ng - 1 + a, k = g.ng - 1 + b;
     const bool interior = a >= alo + 1 && a <= ahi && b >= 1 && b <= g.n[2];
     const long long S = g.s[d];
@@ -164,8 +165,9 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
   StatePtr<T> U0, U1;
   lean_regs(ctl, UA, UB, U0, U1);
   const int nf = g.n[2] + 1, nj = g.n[1] + 2;
-  const int alo = win_lo(g), ahi = win_hi(g);   // the window's x rows, one halo row each side
-  const long long total = (long long) (ahi - alo + 2) * nj * nf;
+  // the window's x rows and the halo rows it computes: a - 1 in [win_flo, win_fhi)
+  const int alo = win_lo(g), ahi = win_hi(g), a0 = win_flo(g) + 1;
+  const long long total = (long long) (win_fhi(g) - win_flo(g)) * nj * nf;
   const long long q = (long long) blockIdx.x * 127 - 1 + threadIdx.x;
   T ml = T(0);
   FluxTally ft{0, 0, 0, 0, 0};
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(128, MGPU_FLUX_MINB) k_lean_sweep_z(Grid g, co
     const long long row = q / nf;
     const int fk = (int) (q - row * nf);              // face fk + ng - 1
     const int ar = (int) (row / nj), b = (int) (row - (long long) ar * nj);
-    const int a = alo + ar;
+    const int a = a0 + ar;
     const int i = g.ng - 1 + a, j = g.ng - 1 + b;
     f = (long long) i * g.s[0] + (long long) j * g.s[1] + (g.ng - 1 + fk);
 #pragma unroll
@@ -362,7 +364,7 @@ inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, c
 {
   const unsigned blk = 128;
   if (dim == 3) {
-    const long long total = (long long) (win_rows(g) + 2) * (g.n[1] + 2) * (g.n[2] + 1);
+    const long long total = (long long) (win_fhi(g) - win_flo(g)) * (g.n[1] + 2) * (g.n[2] + 1);
     const unsigned grid = (unsigned) ((total + 126) / 127);
 #define MGPU_LEANZ_CASE(R) \
   if (rs == R) { k_lean_sweep_z<T, R><<<grid, blk, 0, st>>>(g, PA, UA, UB, Bf, c, pp, ctl, s); return; }
@@ -373,7 +375,7 @@ inline void launch_lean_sweep(const Grid &g, int dim, int rs, cudaStream_t st, c
   // x sweep: columns over (y, z), marching over the window's rows; y sweep: columns over the
   // window's rows (one halo row each side) and z, marching over y
   const long long ncol = dim == 1 ? (long long) (g.n[1] + 2) * (g.n[2] + 2)
-                                  : (long long) (win_rows(g) + 2) * (g.n[2] + 2);
+                                  : (long long) (win_fhi(g) - win_flo(g)) * (g.n[2] + 2);
   const int nmarch = dim == 1 ? win_rows(g) : g.n[1];
   const int L = lean_chunk(ncol, nmarch, 148ll * MGPU_FLUX_MINB * blk);
   const long long nchunk = (nmarch + L - 1) / L;

@@ -122,14 +122,19 @@ struct Grid {
   const int *mult[3];
   // Window of the lean-layout launches: interior x rows [w0, w1) (w1 == 0: all rows).  A
   // window's launches read the rows within the stencil's reach around it and write only its
-  // own rows (plus one halo row each side of the face fields, with the values the
-  // neighbouring window writes there too).
-  int w0, w1;
+  // own rows, plus one halo row each side of the y and z face fields (the values the
+  // neighbouring window writes there too).  whskip bit 0 / bit 1 leaves out the lower / upper
+  // halo row, when the neighbouring window has already written it.
+  int w0, w1, whskip;
 };
 
 __host__ __device__ inline int win_lo(const Grid &g) { return g.w1 ? g.w0 : 0; }
 __host__ __device__ inline int win_hi(const Grid &g) { return g.w1 ? g.w1 : g.n[0]; }
 __host__ __device__ inline int win_rows(const Grid &g) { return win_hi(g) - win_lo(g); }
+// The x rows (interior-relative, -1 = the lower guard row) whose y and z face fields the
+// window's sweeps compute: [win_flo, win_fhi)
+__host__ __device__ inline int win_flo(const Grid &g) { return win_lo(g) - 1 + (g.whskip & 1); }
+__host__ __device__ inline int win_fhi(const Grid &g) { return win_hi(g) + 1 - ((g.whskip >> 1) & 1); }
 // The window's interior flat indices: [win_tbeg, win_tend)
 __host__ __device__ inline long long win_tbeg(const Grid &g) { return (long long) win_lo(g) * g.n[1] * g.n[2]; }
 __host__ __device__ inline long long win_tend(const Grid &g) { return (long long) win_hi(g) * g.n[1] * g.n[2]; }

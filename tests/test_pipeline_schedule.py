@@ -6,9 +6,11 @@ holds (stage v lives in array (v + K) % 2, so the closing c2p's in the solver's 
 stage's sum the Runge-Kutta register holds.  Each operation asserts that every row it reads
 holds the version it needs -- not yet written (a read before the producer) and already
 overwritten (a write before the last reader) both fail -- and then writes its own rows.
-Rows are periodic in x (the end slabs' guard images are their neighbours' rows).  A sweep
-reads the stage primitives up to three rows beyond its slab (WENO5); the face fields CT reads
-one row beyond the slab are written by the same operation's sweeps, so they need no check.
+Rows of primitives are periodic in x (the end slabs' guard images are their neighbours'
+rows).  A sweep reads the stage primitives up to three rows beyond its slab (WENO5).  CT reads
+the y and z face fields one row beyond its slab: the same operation's sweeps compute those halo
+rows, except the one next to the neighbour toward slab 0, whose sweeps computed it as their own
+row (face fields have no periodic images: rows -1 and n0 are guard rows of their own).
 """
 import ctypes
 
@@ -64,15 +66,26 @@ def simulate(S, K, n0):
     return finished
 
 
+def pred(S, s):
+    """The neighbour whose same-stage sweeps computed one of this slab's halo rows."""
+    if 1 <= s <= S // 2:
+        return s - 1
+    if S // 2 < s <= S - 2:
+        return s + 1
+    return None
+
+
 def dependencies(S, K, s, e):
-    """The operations that (s, e) waits for: the slab's previous one, and for sweeps (odd e
-    below the download) the neighbours' previous ones."""
+    """The operations that (s, e) waits for: the slab's previous one; for sweeps (odd e below
+    the download) the neighbours' previous ones and the sweeps of pred(s)."""
     E = 2 * K + 2
     if e == 0:
         return []
     deps = [(s, e - 1)]
     if e % 2 == 1 and e != E - 1:
         deps += [((s - 1) % S, e - 1), ((s + 1) % S, e - 1)]
+        if pred(S, s) is not None:
+            deps.append((pred(S, s), e))
     return deps
 
 
@@ -95,6 +108,16 @@ def check_dag(S, K, n0):
 
     def rows(s, ext=0):
         return [r % n0 for r in range(wb[s] - ext, wb[s + 1] + ext)]
+
+    def face_rows(s):
+        """Rows of y/z face fields this slab's sweeps write (unwrapped: -1 and n0 are guards)."""
+        lo, hi = wb[s] - 1, wb[s + 1] + 1
+        p = pred(S, s)
+        if p == s - 1:
+            lo += 1
+        elif p == s + 1:
+            hi -= 1
+        return list(range(lo, hi))
 
     def done_before(x, op):
         return x == op or x in anc[op]
@@ -137,8 +160,8 @@ def check_dag(S, K, n0):
             if k > 0:
                 read(op, "u1", own, k - 1)
             write(op, "u1", own, k)
-            write(op, "bf", rows(s, 1), k, same_value_ok=True)
-            read(op, "bf", rows(s, 1), k)
+            write(op, "bf", face_rows(s), k, same_value_ok=True)
+            read(op, "bf", list(range(wb[s] - 1, wb[s + 1] + 1)), k)
         else:
             k = e // 2
             read(op, "u1", own, k - 1)

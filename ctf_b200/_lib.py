@@ -78,6 +78,7 @@ SIGNATURES = {
     "mgpu_set_pipeline": (ctypes.c_int, [_vp, ctypes.c_int]),
     "mgpu_get_pipeline": (ctypes.c_int, [_vp, _ip, _ip]),
     "mgpu_pipeline_schedule": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int]),
+    "mgpu_pipeline_bounds": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int]),
     "mgpu_advance_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double]),
     "mgpu_synchronize": (ctypes.c_int, [_vp]),

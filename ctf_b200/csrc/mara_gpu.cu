@@ -609,22 +609,60 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
 // copy-in buffer and go back when the advance does not commit.  A pageable buffer is written
 // after the commit only (its copies would block the host thread).
 
-// Slabs of the pipelined host advance for this solver (0: run unpipelined).
-static int pipe_slab_count(const mgpu_solver *h)
+// Slab boundaries of the pipelined host advance over n0 interior x rows: wb[0..S] (slab s is
+// rows [wb[s], wb[s+1])), or nothing when n0 is too small (at least 3 slabs of 4 rows, deeper
+// than any stencil's reach).  slabs > 0: that many equal slabs.  Automatic (-1): below 96 rows,
+// slabs of about 11 rows; from 96 rows, slabs of 16 rows except thin ones of 6 rows around slab
+// 0 and around the far side uploaded last.  The thin slabs start the pipeline after fewer rows
+// have arrived and shorten the work and the copies out that follow the last copy in; the thick
+// ones recompute fewer halo rows of face fields.
+static std::vector<int> pipe_bounds(int n0, int slabs)
+{
+  std::vector<int> wb;
+  const int smax = n0 / 4;
+  if (smax < 3) return wb;
+  if (slabs > 0 || n0 < 96) {
+    int S = slabs > 0 ? slabs : n0 / 11;
+    S = S < 3 ? 3 : (S > smax ? smax : S);
+    for (int s = 0; s <= S; ++s) wb.push_back((int) ((long long) n0 * s / S));
+    return wb;
+  }
+  const int thin_w = 6, thick_w = 16;
+  auto thin = [](int S, int s) {
+    const int d = s < S - s ? s : S - s;   // ring distance from slab 0
+    return d <= 1 || d >= S / 2 - 3;
+  };
+  auto total = [&](int S) {
+    int t = 0;
+    for (int s = 0; s < S; ++s) t += thin(S, s) ? thin_w : thick_w;
+    return t;
+  };
+  int S = 3;
+  while (total(S + 1) <= n0) ++S;
+  std::vector<int> w(S);
+  int nthick = 0;
+  for (int s = 0; s < S; ++s) {
+    w[s] = thin(S, s) ? thin_w : thick_w;
+    nthick += !thin(S, s);
+  }
+  for (int rem = n0 - total(S), s = 0; rem > 0; s = (s + 1) % S)   // the rows left over
+    if (!thin(S, s) || nthick == 0) {
+      ++w[s];
+      --rem;
+    }
+  wb.push_back(0);
+  for (int s = 0; s < S; ++s) wb.push_back(wb.back() + w[s]);
+  return wb;
+}
+
+// Slab boundaries for this solver's pipelined host advance (empty: run unpipelined).
+static std::vector<int> pipe_slab_bounds(const mgpu_solver *h)
 {
   const Grid &g = h->g;
   if (h->pipe_slabs == 0 || !lean(h) || g.nd != 3 || g.ext[0] || g.ext[1] || g.ext[2] || h->driving ||
       h->prof_on)
-    return 0;
-  const int smax = g.n[0] / 4;   // at least 4 rows per slab: deeper than any stencil's reach
-  if (smax < 3) return 0;
-  // automatic: about 11 rows per slab (measured on a 512^3 box: 16, 24, 32, 48 and 64 slabs
-  // take 352, 324, 314, 309 and 314 ms per call; thinner slabs shorten the copy-out tail after
-  // the last copy in, thicker ones recompute fewer halo rows of face fields)
-  int S = h->pipe_slabs > 0 ? h->pipe_slabs : g.n[0] / 11;
-  if (S < 3) S = 3;
-  if (S > smax) S = smax;
-  return S;
+    return {};
+  return pipe_bounds(g.n[0], h->pipe_slabs);
 }
 
 // Device buffers, streams and events of the pipeline; 1 when device memory does not allow it.
@@ -724,8 +762,9 @@ static std::vector<std::pair<int, int>> pipe_schedule(int S, int K)
   return out;
 }
 
-static int pipe_advance_host(mgpu_solver *h, double *host, double dt, int S, int *errors)
+static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std::vector<int> &wb, int *errors)
 {
+  const int S = (int) wb.size() - 1;
   const Grid &g = h->g;
   const int K = num_stages(h->cfg.rk);
   const int E = 2 * K + 2;   // operations per slab
@@ -734,8 +773,6 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, int S, int
   cudaPointerAttributes pa{};
   const bool pinned = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
   cudaGetLastError();   // an unregistered pointer may leave an error behind
-  std::vector<int> wb(S + 1);
-  for (int s = 0; s <= S; ++s) wb[s] = (int) ((long long) g.n[0] * s / S);
   cudaEvent_t *ev_in = h->pipe_ev.data(), *ev_dl = h->pipe_ev.data() + S;
   const AdvanceArgs A = advance_args(h, 0, dt, 0.0);
   // the primitives of stage v (v = K: the closing c2p's) live in buf(v), the last in the
@@ -838,6 +875,17 @@ int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs)
   return MGPU_OK;
 }
 
+int mgpu_pipeline_bounds(int n0, int slabs, int *bounds, int capacity)
+{
+  if (n0 < 0 || slabs < -1 || slabs == 0 || slabs == 1 || slabs == 2 || capacity < 0) return -MGPU_ERR_ARG;
+  const std::vector<int> wb = pipe_bounds(n0, slabs);
+  if (bounds) {
+    if (capacity < (int) wb.size()) return -MGPU_ERR_ARG;
+    for (size_t i = 0; i < wb.size(); ++i) bounds[i] = wb[i];
+  }
+  return wb.empty() ? 0 : (int) wb.size() - 1;
+}
+
 int mgpu_pipeline_schedule(int slabs, int stages, int *out, int capacity)
 {
   if (slabs < 3 || stages < 1 || stages > 3 || capacity < 0) return -MGPU_ERR_ARG;
@@ -859,11 +907,12 @@ int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps,
   if (!host_aos) return fail(h, MGPU_ERR_ARG, "null primitive buffer");
   const auto t0 = std::chrono::steady_clock::now();
   int err = 0;
-  const int S = pipe_slab_count(h);
+  const std::vector<int> wb = pipe_slab_bounds(h);
+  const int S = wb.empty() ? 0 : (int) wb.size() - 1;
   h->pipe_last = 0;
   if (S && pipe_setup(h, S) == 0) {
     h->pipe_last = S;
-    rc = pipe_advance_host(h, host_aos, dt, S, &err);
+    rc = pipe_advance_host(h, host_aos, dt, wb, &err);
     if (rc) return rc;
   } else {
     rc = mgpu_upload_prim(h, host_aos);

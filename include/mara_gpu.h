@@ -133,8 +133,8 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors);
  * advance's stages and the copy out of different slabs overlap.  The result is the same as the unpipelined call's, bit for bit, and
  * when the advance fails the buffer gets its original contents back. */
 int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors);
-/* Slab count of the pipelined mgpu_advance_host: 0 off, -1 automatic (the default: about 11
- * rows per slab), >= 3 that many (at least 4 x rows each).  *last_slabs (may be NULL) gets the
+/* Slab count of the pipelined mgpu_advance_host: 0 off, -1 automatic (the default; see
+ * mgpu_pipeline_bounds), >= 3 that many equal slabs (at least 4 x rows each).  *last_slabs (may be NULL) gets the
  * count the previous mgpu_advance_host used, 0 when it ran unpipelined. */
 int mgpu_set_pipeline(mgpu_solver *h, int slabs);
 int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs);
@@ -143,6 +143,11 @@ int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs);
  * sweeps and CT, 2k stage k's c2p -- 2*stages the closing one -- and 2*stages+1 the download).
  * Returns the number of pairs (out may be NULL), or -MGPU_ERR_ARG.  Needs no GPU. */
 int mgpu_pipeline_schedule(int slabs, int stages, int *out, int capacity);
+/* The slabs the pipelined advance cuts n0 interior x rows into for a slab setting (-1 or >= 3):
+ * bounds[0..S] (slab s is rows [bounds[s], bounds[s+1])).  Automatic: from 96 rows, slabs of 16
+ * rows and thin ones of 6 around slab 0 and around the far side; below, about 11 rows each.
+ * Returns S (0: too few rows to pipeline; bounds may be NULL), or -MGPU_ERR_ARG.  Needs no GPU. */
+int mgpu_pipeline_bounds(int n0, int slabs, int *bounds, int capacity);
 /* Enqueue n advances without host synchronisation: dt_mode 0 uses `dt` for every step,
  * dt_mode 1 takes each step's dt = cfl*min_dx/MaxLambda of the step before (the first step
  * uses the MaxLambda left by the previous advance).  A step that fails is not committed;

@@ -31,10 +31,20 @@ def schedule(S, K):
     return [(out[2 * i], out[2 * i + 1]) for i in range(n)]
 
 
-def simulate(S, K, n0):
+def bounds(n0, slabs=-1):
+    lib = _lib.load()
+    S = lib.mgpu_pipeline_bounds(n0, slabs, None, 0)
+    if S == 0:
+        return []
+    out = (ctypes.c_int * (S + 1))()
+    assert lib.mgpu_pipeline_bounds(n0, slabs, out, S + 1) == S
+    return list(out)
+
+
+def simulate(S, K, n0, wb=None):
     """Runs the schedule against the row model; returns the order the slabs finished in."""
     E = 2 * K + 2
-    wb = [n0 * s // S for s in range(S + 1)]
+    wb = wb or [n0 * s // S for s in range(S + 1)]
     pa = np.full((2, n0), -1)  # stage of the primitives in each stage array (-1: none yet)
     reg = np.full(n0, -1)      # last stage whose sweeps were added into the register
     finished = []
@@ -89,13 +99,14 @@ def dependencies(S, K, s, e):
     return deps
 
 
-def check_dag(S, K, n0):
+def check_dag(S, K, n0, wb=None):
     """Every hazard ordered by the dependency graph alone, not only by the issue order (so the
     operations could also run on several streams): a read's producer and a write's previous
-    writer and readers are ancestors.  Face fields: a sweep operation writes its own rows and one halo row each side,
-    then CT reads them; two writers of the same stage's face fields write the same values."""
+    writer and readers are ancestors.  Face fields: a sweep operation writes its own rows and
+    the halo rows it computes, then CT reads its rows and one halo row each side; two writers
+    of the same stage's face fields write the same values."""
     E = 2 * K + 2
-    wb = [n0 * s // S for s in range(S + 1)]
+    wb = wb or [n0 * s // S for s in range(S + 1)]
     anc = {}
     for op in schedule(S, K):
         a = set()
@@ -167,6 +178,29 @@ def check_dag(S, K, n0):
             read(op, "u1", own, k - 1)
             read(op, pa(k - 1), own, k - 1)
             write(op, pa(k), own, k)
+
+
+@pytest.mark.parametrize("n0", [12, 16, 24, 95, 96, 128, 256, 512, 1024])
+def test_automatic_slabs(n0):
+    """The automatic slabs cover the rows, at least 4 each, at least 3 of them; from 96 rows
+    thin ones lie around slab 0 and around the far side; and every hazard is ordered."""
+    wb = bounds(n0)
+    S = len(wb) - 1
+    assert S >= 3 and wb[0] == 0 and wb[-1] == n0
+    w = np.diff(wb)
+    assert (w >= 4).all()
+    if n0 >= 96:
+        assert w[0] == w[1] == w[-1] == 6 and w[S // 2] == 6 and w.max() >= 16
+    for K in (1, 2, 3):
+        assert sorted(simulate(S, K, n0, wb)) == list(range(S))
+        check_dag(S, K, n0, wb)
+
+
+def test_fixed_slabs_are_equal():
+    assert bounds(512, 46) == [512 * s // 46 for s in range(47)]
+    assert bounds(11) == [] and bounds(512, 200) == [512 * s // 128 for s in range(129)]
+    lib = _lib.load()
+    assert lib.mgpu_pipeline_bounds(512, 2, None, 0) < 0 and lib.mgpu_pipeline_bounds(512, 0, None, 0) < 0
 
 
 @pytest.mark.parametrize("K", [1, 2, 3])

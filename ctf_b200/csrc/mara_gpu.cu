@@ -609,6 +609,13 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
 // copy-in buffer and go back when the advance does not commit.  A pageable buffer is written
 // after the commit only (its copies would block the host thread).
 
+#ifndef MGPU_PIPE_THIN
+#define MGPU_PIPE_THIN 6     // rows of the thin slabs of the automatic layout
+#endif
+#ifndef MGPU_PIPE_THICK
+#define MGPU_PIPE_THICK 16   // rows of the others
+#endif
+
 // Slab boundaries of the pipelined host advance over n0 interior x rows: wb[0..S] (slab s is
 // rows [wb[s], wb[s+1])), or nothing when n0 is too small (at least 3 slabs of 4 rows, deeper
 // than any stencil's reach).  slabs > 0: that many equal slabs.  Automatic (-1): below 96 rows,
@@ -627,7 +634,7 @@ static std::vector<int> pipe_bounds(int n0, int slabs)
     for (int s = 0; s <= S; ++s) wb.push_back((int) ((long long) n0 * s / S));
     return wb;
   }
-  const int thin_w = 6, thick_w = 16;
+  const int thin_w = MGPU_PIPE_THIN, thick_w = MGPU_PIPE_THICK;
   auto thin = [](int S, int s) {
     const int d = s < S - s ? s : S - s;   // ring distance from slab 0
     return d <= 1 || d >= S / 2 - 3;

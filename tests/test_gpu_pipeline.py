@@ -97,6 +97,15 @@ def test_pipelined_fp64_and_learned():
     _same(_run(P0, n, 0, dts, True, "fp32", True, **kw), _run(P0, n, 4, dts, True, "fp32", True, **kw), 4)
 
 
+def test_automatic_uneven_slabs():
+    """From 96 x rows the automatic layout mixes 6-row and 16-row slabs (12 at 96 rows)."""
+    n = (96, 12, 10)
+    kw = dict(extrap="plm", riemann="hlld", advance="rk3")
+    P0 = ics.turbulence_box(n, seed=37, vrms=0.3)
+    dts = _dts(P0, n, **kw)
+    _same(_run(P0, n, 0, dts, True, **kw), _run(P0, n, -1, dts, True, **kw), 12)
+
+
 def test_default_pipeline_and_standard_layout():
     n = (16, 16, 16)
     P0 = ics.turbulence_box(n, seed=3, vrms=0.2)

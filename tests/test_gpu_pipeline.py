@@ -97,6 +97,20 @@ def test_pipelined_fp64_and_learned():
     _same(_run(P0, n, 0, dts, True, "fp32", True, **kw), _run(P0, n, 4, dts, True, "fp32", True, **kw), 4)
 
 
+@pytest.mark.parametrize("learned", [False, True])
+def test_pipelined_stress_box_with_emergency_reset(learned):
+    """The stress box with the emergency reset: zones fail and are reset in every step, a path
+    that amplifies any difference in the last bits, and the state is still the same bit for
+    bit."""
+    n = (16, 16, 16)
+    kw = dict(extrap="plm", riemann="hlld", advance="rk3", ereset=True, preset=0.01, dreset=1.0)
+    P0 = ics.stress_box(n, seed=0)
+    dts = _dts(P0, n, **kw)
+    a = _run(P0, n, 0, dts, True, "fp32", learned, **kw)
+    _same(a, _run(P0, n, 4, dts, True, "fp32", learned, **kw), 4)
+    assert a[0][3]["c2p_failed"] > 0
+
+
 def test_automatic_uneven_slabs():
     """From 96 x rows the automatic layout mixes 6-row and 16-row slabs (12 at 96 rows)."""
     n = (96, 12, 10)

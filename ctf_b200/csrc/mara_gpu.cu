@@ -20,6 +20,7 @@ MGPU_DECLARE_PRECISION(fp32)
 using namespace mgpu;
 
 #include "solver.h"
+#include "host_copy.h"
 #include "measures.h"
 
 namespace {
@@ -73,9 +74,14 @@ void pipe_free(mgpu_solver *h, bool streams)
   h->pipe_in = h->pipe_out = nullptr;
   h->pipe_guess = h->pipe_pa = nullptr;
   h->pipe_state = 0;
+  if (h->pipe_host) cudaFreeHost(h->pipe_host);
+  h->pipe_host = nullptr;
+  h->pipe_host_state = 0;
   if (!streams) return;
   for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
   h->pipe_ev.clear();
+  delete h->pipe_pool;
+  h->pipe_pool = nullptr;
   if (h->pipe_h2d) cudaStreamDestroy(h->pipe_h2d);
   if (h->pipe_d2h) cudaStreamDestroy(h->pipe_d2h);
   h->pipe_h2d = h->pipe_d2h = nullptr;
@@ -708,7 +714,7 @@ static int pipe_setup(mgpu_solver *h, int S)
   }
   if (!h->pipe_h2d) CK(cudaStreamCreateWithFlags(&h->pipe_h2d, cudaStreamNonBlocking));
   if (!h->pipe_d2h) CK(cudaStreamCreateWithFlags(&h->pipe_d2h, cudaStreamNonBlocking));
-  while ((int) h->pipe_ev.size() < 2 * S) {
+  while ((int) h->pipe_ev.size() < 3 * S) {
     cudaEvent_t e;
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     h->pipe_ev.push_back(e);
@@ -769,6 +775,29 @@ static std::vector<std::pair<int, int>> pipe_schedule(int S, int K)
   return out;
 }
 
+// The pinned staging copy of the AoS buffer and the copy threads, for a pageable caller
+// buffer; false when pinned host memory of that size cannot be had (the copies then go to the
+// pageable buffer directly, the copy out after the commit).
+static bool pipe_host_setup(mgpu_solver *h)
+{
+  if (h->pipe_host_state == 0) {
+    if (cudaHostAlloc((void **) &h->pipe_host, (size_t) h->g.nz * 8 * sizeof(double), cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      h->pipe_host = nullptr;
+      h->pipe_host_state = -1;
+      return false;
+    }
+    h->pipe_host_state = 1;
+  }
+  if (h->pipe_host_state < 0) return false;
+  if (!h->pipe_pool) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    h->pipe_pool = new HostCopyPool(hc >= 16 ? 8 : (hc >= 2 ? (int) hc / 2 : 1));
+  }
+  return true;
+}
+
 static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std::vector<int> &wb, int *errors)
 {
   const int S = (int) wb.size() - 1;
@@ -780,7 +809,13 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std:
   cudaPointerAttributes pa{};
   const bool pinned = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
   cudaGetLastError();   // an unregistered pointer may leave an error behind
-  cudaEvent_t *ev_in = h->pipe_ev.data(), *ev_dl = h->pipe_ev.data() + S;
+  // a pageable buffer goes through the pinned staging copy: the DMA copies read and write
+  // `dma`, and the pool copies between it and the caller's buffer
+  const bool staged = !pinned && pipe_host_setup(h);
+  double *dma = staged ? h->pipe_host : host;
+  const bool early_out = pinned || staged;   // copies out while later slabs compute
+  cudaEvent_t *ev_in = h->pipe_ev.data(), *ev_dl = ev_in + S, *ev_out = ev_in + 2 * S;
+  std::vector<int> out_order;   // slabs in the order of their copies out
   const AdvanceArgs A = advance_args(h, 0, dt, 0.0);
   // the primitives of stage v (v = K: the closing c2p's) live in buf(v), the last in the
   // solver's own PA
@@ -828,7 +863,8 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std:
     if (e == 0) {
       // the copy in: the slab's rows, and the end slabs' guard rows (kept for the restore)
       const long long r0 = s == 0 ? 0 : ng + wb[s], r1 = s == S - 1 ? G0 : ng + wb[s + 1];
-      CK(copy_rows(h->pipe_in, host, r0, r1, cudaMemcpyHostToDevice, h->pipe_h2d));
+      if (staged) h->pipe_pool->copy(dma + r0 * s0 * 8, host + r0 * s0 * 8, (size_t) ((r1 - r0) * row_bytes));
+      CK(copy_rows(h->pipe_in, dma, r0, r1, cudaMemcpyHostToDevice, h->pipe_h2d));
       CK(cudaEventRecord(ev_in[s], h->pipe_h2d));
       CK(cudaStreamWaitEvent(h->stream, ev_in[s], 0));
       const long long z0 = (ng + wb[s]) * s0, cnt = (long long) (wb[s + 1] - wb[s]) * s0;
@@ -837,11 +873,13 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std:
       long long r[3][2];
       const int n = out_ranges(s, r);
       for (int i = 0; i < n; ++i) CK(download_rows(r[i][0], r[i][1]));
-      if (pinned) {
+      if (early_out) {
         CK(cudaEventRecord(ev_dl[s], h->stream));
         CK(cudaStreamWaitEvent(h->pipe_d2h, ev_dl[s], 0));
         for (int i = 0; i < n; ++i)
-          CK(copy_rows(host, h->pipe_out, r[i][0], r[i][1], cudaMemcpyDeviceToHost, h->pipe_d2h));
+          CK(copy_rows(dma, h->pipe_out, r[i][0], r[i][1], cudaMemcpyDeviceToHost, h->pipe_d2h));
+        CK(cudaEventRecord(ev_out[s], h->pipe_d2h));
+        out_order.push_back(s);
       }
     } else if (e % 2 == 1) {
       CK(phase(window(s, (e - 1) / 2), PH_FLUX_UPDATE, (e - 1) / 2));
@@ -851,16 +889,27 @@ static int pipe_advance_host(mgpu_solver *h, double *host, double dt, const std:
   }
   CK(phase(A, PH_COMMIT, 0));
   CK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  if (staged) {   // each slab's result from the staging copy into the caller's buffer as it lands
+    for (int s : out_order) {
+      CK(cudaEventSynchronize(ev_out[s]));
+      long long r[3][2];
+      const int n = out_ranges(s, r);
+      for (int i = 0; i < n; ++i)
+        h->pipe_pool->copy(host + r[i][0] * s0 * 8, dma + r[i][0] * s0 * 8, (size_t) ((r[i][1] - r[i][0]) * row_bytes));
+    }
+  }
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaStreamSynchronize(h->pipe_d2h));
   CK(cudaStreamSynchronize(h->pipe_h2d));
   if (h->ctl_host->tc_fault) return fail(h, MGPU_ERR_CUDA, "a tensor-core wait of the learned c2p timed out");
   const int err = errors_of(*h->ctl_host, h->cfg.rk);
-  if (pinned && err) {          // the copies out went ahead: put the caller's buffer back
-    CK(cudaMemcpyAsync(host, h->pipe_in, (size_t) g.nz * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  const size_t all = (size_t) g.nz * 8 * sizeof(double);
+  if (early_out && err) {       // the copies out went ahead: put the caller's buffer back
+    CK(cudaMemcpyAsync(dma, h->pipe_in, all, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-  } else if (!pinned && !err) {
-    CK(cudaMemcpyAsync(host, h->pipe_out, (size_t) g.nz * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (staged) h->pipe_pool->copy(host, dma, all);
+  } else if (!early_out && !err) {
+    CK(cudaMemcpyAsync(host, h->pipe_out, all, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
   }
   *errors = err;

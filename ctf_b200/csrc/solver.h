@@ -8,6 +8,7 @@
 #include "rmhd_types.cuh"
 
 struct MgpuDriving;   // OU driving field (driving.cu)
+class HostCopyPool;   // threaded host copies (host_copy.h)
 
 struct mgpu_solver {
   mgpu_config cfg;
@@ -52,6 +53,11 @@ struct mgpu_solver {
   void *pipe_guess = nullptr, *pipe_pa = nullptr;
   cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
   std::vector<cudaEvent_t> pipe_ev;
+  // a pageable caller buffer is staged through this pinned copy of the AoS buffer, its host
+  // copies spread over the pool's threads (0 / -1: not set up / not available)
+  double *pipe_host = nullptr;
+  int pipe_host_state = 0;
+  HostCopyPool *pipe_pool = nullptr;
 };
 
 

@@ -130,12 +130,15 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors);
  * errors == 0; *kzps is 1e-3 * zones (guards included) / wall seconds of the call.
  * In the 3-D lean layout the call is pipelined over slabs of x rows when device memory allows
  * (two device copies of the AoS buffer and a second stage-primitive array): the copy in, the
- * advance's stages and the copy out of different slabs overlap.  The result is the same as the unpipelined call's, bit for bit, and
- * when the advance fails the buffer gets its original contents back. */
+ * advance's stages and the copy out of different slabs overlap.  The result is the same as
+ * the unpipelined call's, bit for bit, and when the advance fails the buffer gets its original
+ * contents back.  A pageable buffer is staged through a pinned host copy that the solver
+ * allocates on its first such call, with the host copies on a few threads of its own. */
 int mgpu_advance_host(mgpu_solver *h, double *host_aos, double dt, double *kzps, int *errors);
 /* Slab count of the pipelined mgpu_advance_host: 0 off, -1 automatic (the default; see
- * mgpu_pipeline_bounds), >= 3 that many equal slabs (at least 4 x rows each).  *last_slabs (may be NULL) gets the
- * count the previous mgpu_advance_host used, 0 when it ran unpipelined. */
+ * mgpu_pipeline_bounds), >= 3 that many equal slabs (at least 4 x rows each).  *last_slabs
+ * (may be NULL) gets the count the previous mgpu_advance_host used, 0 when it ran
+ * unpipelined. */
 int mgpu_set_pipeline(mgpu_solver *h, int slabs);
 int mgpu_get_pipeline(const mgpu_solver *h, int *slabs, int *last_slabs);
 /* The pipelined advance's issue order for `slabs` slabs and `stages` Runge-Kutta stages, as

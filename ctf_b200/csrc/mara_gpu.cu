@@ -82,6 +82,8 @@ void pipe_free(mgpu_solver *h, bool streams)
   h->pipe_ev.clear();
   delete h->pipe_pool;
   h->pipe_pool = nullptr;
+  for (cudaEvent_t e : h->xfer_ev) cudaEventDestroy(e);
+  h->xfer_ev.clear();
   if (h->pipe_h2d) cudaStreamDestroy(h->pipe_h2d);
   if (h->pipe_d2h) cudaStreamDestroy(h->pipe_d2h);
   h->pipe_h2d = h->pipe_d2h = nullptr;
@@ -445,6 +447,8 @@ int mgpu_num_zones(const mgpu_solver *h, long long *nz)
   return MGPU_OK;
 }
 
+static bool pipe_host_setup(mgpu_solver *h);
+
 static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_out, int kind, long long zbeg = 0,
                     long long zcount = -1)
 {
@@ -473,11 +477,23 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
     CK(cudaStreamSynchronize(h->stream));
     return MGPU_OK;
   }
+  // a large pageable buffer goes through the pinned staging copy (pipe_host), chunk by chunk:
+  // the threaded host copy of one chunk overlaps the DMA copy and conversion of the previous
+  bool staged = false;
+  if ((size_t) (nz - zbeg) * 8 * sizeof(double) >= (size_t(64) << 20)) {
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, host + zbeg * 8) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();   // an unregistered pointer may leave an error behind
+    staged = !pinned && pipe_host_setup(h);
+  }
+  double *dma = staged ? h->pipe_host : host;
+  int nchunk = 0;
   for (long long z0 = zbeg; z0 < nz; z0 += h->staging_zones) {
     const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
     const size_t bytes = (size_t) cnt * 8 * sizeof(double);
     if (upload) {
-      CK(cudaMemcpyAsync(h->staging, host + z0 * 8, bytes, cudaMemcpyHostToDevice, h->stream));
+      if (staged) h->pipe_pool->copy(dma + z0 * 8, host + z0 * 8, bytes);
+      CK(cudaMemcpyAsync(h->staging, dma + z0 * 8, bytes, cudaMemcpyHostToDevice, h->stream));
       cudaError_t e = kind == 0 ? (fp32(h) ? upload_fp32(t, h->staging, z0, cnt) : upload_fp64(t, h->staging, z0, cnt))
                                 : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 0)
                                            : face_io_fp64(t, h->staging, z0, cnt, 0));
@@ -488,7 +504,24 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
                                 : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 1)
                                            : face_io_fp64(t, h->staging, z0, cnt, 1));
       CK(e);
-      CK(cudaMemcpyAsync(host + z0 * 8, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(dma + z0 * 8, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+      if (staged) {
+        if ((int) h->xfer_ev.size() <= nchunk) {
+          cudaEvent_t ev;
+          CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+          h->xfer_ev.push_back(ev);
+        }
+        CK(cudaEventRecord(h->xfer_ev[nchunk], h->stream));
+      }
+    }
+    ++nchunk;
+  }
+  if (staged && !upload) {   // each chunk from the staging copy into the caller's buffer as it lands
+    int c = 0;
+    for (long long z0 = zbeg; z0 < nz; z0 += h->staging_zones, ++c) {
+      const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
+      CK(cudaEventSynchronize(h->xfer_ev[c]));
+      h->pipe_pool->copy(host + z0 * 8, dma + z0 * 8, (size_t) cnt * 8 * sizeof(double));
     }
   }
   CK(cudaStreamSynchronize(h->stream));

@@ -58,6 +58,7 @@ struct mgpu_solver {
   double *pipe_host = nullptr;
   int pipe_host_state = 0;
   HostCopyPool *pipe_pool = nullptr;
+  std::vector<cudaEvent_t> xfer_ev;   // per chunk of a staged download (transfer)
 };
 
 

@@ -77,6 +77,9 @@ void pipe_free(mgpu_solver *h, bool streams)
   if (h->pipe_host) cudaFreeHost(h->pipe_host);
   h->pipe_host = nullptr;
   h->pipe_host_state = 0;
+  if (h->xfer_host) cudaFreeHost(h->xfer_host);
+  h->xfer_host = nullptr;
+  h->xfer_host_state = 0;
   if (!streams) return;
   for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
   h->pipe_ev.clear();
@@ -449,6 +452,36 @@ int mgpu_num_zones(const mgpu_solver *h, long long *nz)
 
 static bool pipe_host_setup(mgpu_solver *h);
 
+// Two pinned slots of the device staging chunk's size and two events, for the chunked host
+// transfers of a large pageable buffer, and the copy threads; false when they cannot be had
+// (the copies then read and write the pageable buffer directly).
+static bool xfer_host_setup(mgpu_solver *h)
+{
+  if (h->xfer_host_state == 0) {
+    cudaError_t e = cudaHostAlloc((void **) &h->xfer_host, (size_t) h->staging_zones * 2 * 8 * sizeof(double),
+                                  cudaHostAllocDefault);
+    while (h->xfer_ev.size() < 2 && e == cudaSuccess) {   // the events outlive a new domain
+      cudaEvent_t ev;
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess) h->xfer_ev.push_back(ev);
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      if (h->xfer_host) cudaFreeHost(h->xfer_host);
+      h->xfer_host = nullptr;
+      h->xfer_host_state = -1;
+      return false;
+    }
+    h->xfer_host_state = 1;
+  }
+  if (h->xfer_host_state < 0) return false;
+  if (!h->pipe_pool) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    h->pipe_pool = new HostCopyPool(hc >= 16 ? 8 : (hc >= 2 ? (int) hc / 2 : 1));
+  }
+  return true;
+}
+
 static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_out, int kind, long long zbeg = 0,
                     long long zcount = -1)
 {
@@ -477,23 +510,29 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
     CK(cudaStreamSynchronize(h->stream));
     return MGPU_OK;
   }
-  // a large pageable buffer goes through the pinned staging copy (pipe_host), chunk by chunk:
-  // the threaded host copy of one chunk overlaps the DMA copy and conversion of the previous
+  // a large pageable buffer goes through two pinned chunk slots (xfer_host), chunk by chunk:
+  // the threaded host copy of one chunk overlaps the DMA copy and conversion of the other
   bool staged = false;
   if ((size_t) (nz - zbeg) * 8 * sizeof(double) >= (size_t(64) << 20)) {
     cudaPointerAttributes pa{};
     const bool pinned = cudaPointerGetAttributes(&pa, host + zbeg * 8) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();   // an unregistered pointer may leave an error behind
-    staged = !pinned && pipe_host_setup(h);
+    staged = !pinned && xfer_host_setup(h);
   }
-  double *dma = staged ? h->pipe_host : host;
+  const long long slot_doubles = h->staging_zones * 8;
+  auto slot = [&](int c) { return h->xfer_host + (c % 2) * slot_doubles; };
   int nchunk = 0;
   for (long long z0 = zbeg; z0 < nz; z0 += h->staging_zones) {
     const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
     const size_t bytes = (size_t) cnt * 8 * sizeof(double);
+    double *dma = staged ? slot(nchunk) : host + z0 * 8;   // where this chunk's DMA copy reads or writes
     if (upload) {
-      if (staged) h->pipe_pool->copy(dma + z0 * 8, host + z0 * 8, bytes);
-      CK(cudaMemcpyAsync(h->staging, dma + z0 * 8, bytes, cudaMemcpyHostToDevice, h->stream));
+      if (staged) {
+        if (nchunk >= 2) CK(cudaEventSynchronize(h->xfer_ev[nchunk % 2]));   // the slot's previous copy
+        h->pipe_pool->copy(dma, host + z0 * 8, bytes);
+      }
+      CK(cudaMemcpyAsync(h->staging, dma, bytes, cudaMemcpyHostToDevice, h->stream));
+      if (staged) CK(cudaEventRecord(h->xfer_ev[nchunk % 2], h->stream));
       cudaError_t e = kind == 0 ? (fp32(h) ? upload_fp32(t, h->staging, z0, cnt) : upload_fp64(t, h->staging, z0, cnt))
                                 : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 0)
                                            : face_io_fp64(t, h->staging, z0, cnt, 0));
@@ -504,25 +543,22 @@ static int transfer(mgpu_solver *h, double *host, const void *dev_in, void *dev_
                                 : (fp32(h) ? face_io_fp32(t, h->staging, z0, cnt, 1)
                                            : face_io_fp64(t, h->staging, z0, cnt, 1));
       CK(e);
-      CK(cudaMemcpyAsync(dma + z0 * 8, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(dma, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
       if (staged) {
-        if ((int) h->xfer_ev.size() <= nchunk) {
-          cudaEvent_t ev;
-          CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-          h->xfer_ev.push_back(ev);
+        CK(cudaEventRecord(h->xfer_ev[nchunk % 2], h->stream));
+        if (nchunk >= 1) {   // the previous chunk, from its slot into the caller's buffer
+          const long long zp = z0 - h->staging_zones;
+          CK(cudaEventSynchronize(h->xfer_ev[(nchunk - 1) % 2]));
+          h->pipe_pool->copy(host + zp * 8, slot(nchunk - 1), (size_t) h->staging_zones * 8 * sizeof(double));
         }
-        CK(cudaEventRecord(h->xfer_ev[nchunk], h->stream));
       }
     }
     ++nchunk;
   }
-  if (staged && !upload) {   // each chunk from the staging copy into the caller's buffer as it lands
-    int c = 0;
-    for (long long z0 = zbeg; z0 < nz; z0 += h->staging_zones, ++c) {
-      const long long cnt = (nz - z0) < h->staging_zones ? (nz - z0) : h->staging_zones;
-      CK(cudaEventSynchronize(h->xfer_ev[c]));
-      h->pipe_pool->copy(host + z0 * 8, dma + z0 * 8, (size_t) cnt * 8 * sizeof(double));
-    }
+  if (staged && !upload && nchunk >= 1) {   // the last chunk
+    const long long zl = zbeg + (long long) (nchunk - 1) * h->staging_zones;
+    CK(cudaEventSynchronize(h->xfer_ev[(nchunk - 1) % 2]));
+    h->pipe_pool->copy(host + zl * 8, slot(nchunk - 1), (size_t) (nz - zl) * 8 * sizeof(double));
   }
   CK(cudaStreamSynchronize(h->stream));
   return MGPU_OK;

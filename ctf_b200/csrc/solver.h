@@ -58,7 +58,10 @@ struct mgpu_solver {
   double *pipe_host = nullptr;
   int pipe_host_state = 0;
   HostCopyPool *pipe_pool = nullptr;
-  std::vector<cudaEvent_t> xfer_ev;   // per chunk of a staged download (transfer)
+  // the plain host transfers of a large pageable buffer: two pinned chunk slots and their events
+  double *xfer_host = nullptr;
+  int xfer_host_state = 0;
+  std::vector<cudaEvent_t> xfer_ev;
 };
 
 

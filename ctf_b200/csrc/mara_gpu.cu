@@ -681,8 +681,11 @@ int mgpu_advance(mgpu_solver *h, double dt, int *errors)
 // the latest first.  The copies run on their own streams, so the copy in of later slabs and the
 // copy out of earlier ones overlap the advance.  With a pinned caller buffer the copies out
 // write it before the advance is known to commit; its original contents stay in the device
-// copy-in buffer and go back when the advance does not commit.  A pageable buffer is written
-// after the commit only (its copies would block the host thread).
+// copy-in buffer and go back when the advance does not commit.  A pageable buffer goes through
+// a pinned copy of the AoS buffer (pipe_host_setup) with the same schedule, the pool's threads
+// copying each slab's rows in before its copy in and its result out as its copy out lands;
+// without that pinned copy it is written after the commit only (copies of pageable memory
+// would block the host thread).
 
 #ifndef MGPU_PIPE_THIN
 #define MGPU_PIPE_THIN 6     // rows of the thin slabs of the automatic layout

@@ -53,7 +53,7 @@ class HostCopyPool {
  private:
   void part(int i)
   {
-    const size_t chunk = (bytes_ / n_ + 4095) / 4096 * 4096;
+    const size_t chunk = ((bytes_ + n_ - 1) / n_ + 4095) / 4096 * 4096;   // n_ parts cover every byte
     const size_t b = std::min(bytes_, chunk * (size_t) i), e = std::min(bytes_, b + chunk);
     if (e > b) memcpy(dst_ + b, src_ + b, e - b);
   }

@@ -45,3 +45,27 @@ def test_pageable_transfers_match_pinned(layout, precision):
     assert ea == eb == 0
     assert np.array_equal(pageable, pinned)
     del keep, keep_out
+
+
+def test_pageable_range_transfers_match_pinned():
+    """Ranges that start and end inside the array (mgpu_upload_prim_range,
+    mgpu_download_prim_range): the staged chunks follow the range's first zone."""
+    from ctf_b200.mara import _dp
+    P0 = ics.turbulence_box(N, seed=9, vrms=0.2)
+    a, b = Solver(Scheme(), N), Solver(Scheme(), N)   # FP64, standard layout
+    flat = P0.reshape(-1, 8)
+    z0 = 100_003
+    cnt = flat.shape[0] - z0 - 7                      # 4.47 M zones (286 MB): two chunks
+    R = flat[z0:z0 + cnt].copy()
+    R[:, 0] *= 1.01                                   # a density change, still physical
+    for s in (a, b):
+        s.upload(P0.copy())
+    a.upload_range(R.copy(), z0)                      # pageable: staged
+    keep, pinned = _pinned_like(R)
+    b.upload_range(pinned, z0)                        # pinned: direct
+    assert np.array_equal(a.download(), b.download())
+    keep_out, pinned_out = _pinned_like(np.zeros_like(R))
+    assert b.lib.mgpu_download_prim_range(b.h, _dp(pinned_out), z0, cnt) == 0
+    got = a.download_range(z0, cnt)                   # pageable: staged
+    assert np.array_equal(got, pinned_out) and np.array_equal(got, R)
+    del keep, keep_out

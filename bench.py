@@ -19,6 +19,12 @@ flux differences straight into the Runge-Kutta register, only the transverse fac
 stored; `--layout standard` for the stored-flux layout); the FP64 runs use the standard
 layout, the one held to the reference's golden steps.
 
+`e2e` times the same FP32 + learned solver through Mara.advance(buf, dt) with a pinned host
+buffer: every call copies the whole guarded AoS array in and back out.  In the lean layout that
+call is pipelined over slabs of x rows (the copies overlap the advance; the result is the
+unpipelined call's bit for bit), and `e2e.value_unpipelined` gives the same calls with the
+pipeline switched off.
+
 All precisions advance with the same fixed dt (CFL 0.3 of the primed MaxLambda) so their
 final states are comparable.  Every array (8.9 GB per FP64 state at 512^3) is larger than
 the 126 MB L2, so no flush is needed between steps.  For N > 1 (torchrun) every rank
